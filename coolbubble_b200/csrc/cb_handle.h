@@ -1,0 +1,52 @@
+/* cb_handle.h -- the opaque cb_handle of include/coolbubble_b200.h. */
+#ifndef CB_HANDLE_H
+#define CB_HANDLE_H
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "cb_internal.h"
+#include "coolbubble_b200.h"
+
+namespace cb {
+struct FftState;
+}
+
+struct cb_handle {
+    cb_params p{};
+    cb::StepConst k{};
+    int prec = 0;
+    size_t esz = 8;
+    size_t N = 0;
+    bool expanding = false;
+    cudaStream_t stream = nullptr;
+    /* ping-pong field buffers; cphi / cpi index the current ones */
+    void *phi[2] = {nullptr, nullptr};
+    void *pi[2] = {nullptr, nullptr};
+    int cphi = 0, cpi = 0;
+    void *loc[3] = {nullptr, nullptr, nullptr};   /* Ekin, gradphi, potEnergy */
+    cb::DevState *st = nullptr;
+    double *partials = nullptr;
+    size_t npart = 0;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
+    double t = 0.0;
+    long long steps_done = 0;
+    bool pending = false;   /* drift-first: phi is one drift behind the whole step */
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cb::FftState *fft = nullptr;
+    std::string err;
+};
+
+namespace cb {
+int fail(cb_handle *h, int status, const std::string &msg);
+int cuda_fail(cb_handle *h, cudaError_t e, const char *what);
+int sync(cb_handle *h, const char *what);
+int flush_pending(cb_handle *h);
+int ensure_tmp(cb_handle *h, size_t bytes);
+void destroy_handle(cb_handle *h);
+void free_fft(cb_handle *h);
+}  // namespace cb
+
+#endif

@@ -1,0 +1,93 @@
+/* cb_internal.h -- structures shared by the host glue and the CUDA kernels. */
+#ifndef CB_INTERNAL_H
+#define CB_INTERNAL_H
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace cb {
+
+/* Per-site sums accumulated by the step kernel (factor dxLD applied at the end). */
+enum SumIdx {
+    S_EK = 0,   /* sum 0.5 a_kin^(-2d) pi_{n+1/2}^2     (bubble.cpp:810) */
+    S_EP,       /* sum V(phi_n)                          (808) */
+    S_EG,       /* sum 0.5 |grad_+ phi_n / (a dx)|^2     (794-807) */
+    S_PHI,      /* sum phi_n                             (816) */
+    S_V,        /* sum pi_{n+1/2} a_kin^(-d)             (817) */
+    Q_EK,       /* sums of squares for the spreads       (820-825) */
+    Q_EP,
+    Q_EG,
+    Q_ET,
+    Q_PHI,
+    Q_V,
+    S_EKIN_IN,  /* static background: sum 0.5 pi_{n-1/2}^2, the previous step's raw kinetic sum */
+    NSUM
+};
+
+/* Background state on the device. The last block of each step kernel that
+ * measures sums rewrites it (Friedmann update, bubble.cpp:858-875), so
+ * consecutive launches on one stream chain without the host. */
+struct DevState {
+    /* background at the start of the next step */
+    double a, ap, H, C;
+    double ekin_half_prev;
+    /* coefficients the next step uses */
+    double fl;       /* a^(d-2+alpha)                (bubble.cpp:740) */
+    double fv;       /* a^(d+alpha)                  (741) */
+    double a_kin;    /* a + dt/2 a'                  (765) */
+    double kin_w;    /* 0.5 a_kin^(-2d)              (810) */
+    double vel_w;    /* a_kin^(-d)                   (817) */
+    double adx;      /* a dx                         (794) */
+    double inv_adx;
+    double drift_p;  /* pending drift factor a_half^(-d+alpha) (870); 0: none pending */
+    int adx_pow2;    /* a dx is a power of two: multiplying by 1/(a dx) is exact */
+    int pad0;
+    /* the last measured line (sums times dxLD; *_var = sums of squares times dxLD^2) */
+    double etot, ekin, egrad, epot;
+    double etot_var, ekin_var, egrad_var, epot_var;
+    double avphi, avphi_var, avphip, avphip_var;
+    /* last-block-done ticket and error word */
+    unsigned int counter;
+    int err;
+};
+
+/* Constants of one run, passed by value to every launch. */
+struct StepConst {
+    int d, n;
+    int ni, nj, nk;     /* extents mapped onto (march axis, tile rows, tile columns) */
+    int cz;             /* planes per block along the march axis (d = 3) */
+    double dt;
+    double c2, c3, c4;  /* V'(f) = c2 f - c3 f^2 + c4 f^3, coefficients as bubble.cpp:76 forms them */
+    double v2, v3, v4, dv; /* V(f) = v2 f^2 - v3 f^3 + v4 f^4 + DeltaV (bubble.cpp:71) */
+    double dx, dx2, inv_dx2;
+    int dx2_pow2;
+    double dxLD, mpl;
+    int alpha, expanding;
+    int want_local;
+};
+
+/* Kernel launchers (cb_step.cu). Each returns the cudaError_t of the launch. */
+enum Prec { P_FP64 = 0, P_FP32 = 1 };
+
+cudaError_t launch_step(int prec, const StepConst &k, bool drift_first, bool sums, const void *phi_in,
+                        const void *pi_in, void *phi_out, void *pi_out, void *loc_ek, void *loc_eg, void *loc_ep,
+                        DevState *st, double *partials, cudaStream_t s);
+/* Number of blocks (and so of partial-sum slots) a step launch uses. */
+size_t step_blocks(const StepConst &k);
+
+cudaError_t launch_ic_energies(int prec, const StepConst &k, const void *phi, const void *pi, void *loc_ek,
+                               void *loc_eg, void *loc_ep, DevState *st, double *partials, cudaStream_t s);
+cudaError_t launch_ic_backkick(int prec, const StepConst &k, const void *phi, void *pi, DevState *st,
+                               double *partials, cudaStream_t s);
+size_t ic_blocks(const StepConst &k);
+
+/* phi_out = phi + (dt * pi) * drift_p; then drift_p = 0 (applies a pending drift). */
+cudaError_t launch_flush_drift(int prec, const StepConst &k, const void *phi, const void *pi, void *phi_out,
+                               DevState *st, cudaStream_t s);
+cudaError_t launch_convert(int from_prec, int to_prec, const void *src, void *dst, size_t n, cudaStream_t s);
+
+}  // namespace cb
+
+#endif

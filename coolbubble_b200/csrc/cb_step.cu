@@ -1,0 +1,635 @@
+/* cb_step.cu -- the fused leapfrog step for sm_100a.
+ *
+ * One launch performs one step of Bubble::oneStep (reference
+ * src/bubble.cpp:849-876) over the whole lattice:
+ *
+ *   computeForces (716-743) -> kick (853-856) -> measureEnergies (761-844)
+ *   -> a'/a update (860-865) -> drift (867-870) -> H, C (873-875)
+ *
+ * in a single pass over HBM: each block streams a column of sites along
+ * axis 0 (d = 3), keeps the three planes the axis-0 stencil needs in
+ * registers, stages the in-plane tile plus its one-site periodic halo in
+ * shared memory, and writes phi and pi once. The periodic neighbour
+ * arithmetic of gridfuncs.cpp:31-51 becomes wrapped tile coordinates.
+ *
+ * Energy sums are accumulated per thread (double for FP64; compensated
+ * float for FP32C), reduced per warp by shuffles and per block in shared
+ * memory, written as one partial per block, and the last block to finish
+ * (ticket counter) adds the partials in a fixed order in double and applies
+ * the Friedmann update of the background on the device. The result is
+ * deterministic: it does not depend on which block finishes last.
+ *
+ * Two orderings of the leapfrog:
+ *   drift-last  (static background): read phi_n, pi_{n-1/2}; write
+ *               phi_{n+1} = phi_n + dt pi_{n+1/2}, pi_{n+1/2}. No global
+ *               dependency inside a step.
+ *   drift-first (expanding background): the drift of step n needs a_{n+1/2},
+ *               which needs this step's global sums. The stored state is
+ *               (phi_n, pi_{n+1/2}) plus a pending drift factor; the next
+ *               launch applies phi_{n+1} = phi_n + (dt pi_{n+1/2}) p on load
+ *               (for the halo too) before its force. Same bytes per step.
+ *
+ * FP64 arithmetic is written with explicitly rounded operations (no FMA
+ * contraction) in the order the reference evaluates each expression, so the
+ * per-site results differ from the CPU only where CUDA's pow differs from
+ * glibc's (the cubes and fourth powers below are formed as a double-double
+ * square rounded once).
+ */
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <type_traits>
+
+#include "cb_internal.h"
+
+namespace cb {
+
+namespace {
+
+template <typename T>
+struct Ar;
+
+template <>
+struct Ar<double> {
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    static __device__ __forceinline__ double sq(double x) { return __dmul_rn(x, x); }
+    /* x^3 and x^4 from the exact square p + e (Dekker's two-product through an fma), rounded once */
+    static __device__ __forceinline__ double cube(double x) {
+        double p = __dmul_rn(x, x);
+        double e = __fma_rn(x, x, -p);
+        return __fma_rn(p, x, __dmul_rn(e, x));
+    }
+    static __device__ __forceinline__ double quart(double x) {
+        double p = __dmul_rn(x, x);
+        double e = __fma_rn(x, x, -p);
+        return __fma_rn(p, p, __dmul_rn(__dadd_rn(p, p), e));
+    }
+};
+
+template <>
+struct Ar<float> {
+    static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
+    static __device__ __forceinline__ float add(float a, float b) { return a + b; }
+    static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
+    static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+    static __device__ __forceinline__ float sq(float x) { return x * x; }
+    static __device__ __forceinline__ float cube(float x) { return x * x * x; }
+    static __device__ __forceinline__ float quart(float x) { float p = x * x; return p * p; }
+};
+
+/* Per-thread accumulator: double for FP64, Kahan-compensated float for FP32C. */
+template <typename T>
+struct Acc;
+
+template <>
+struct Acc<double> {
+    double s = 0.0;
+    __device__ __forceinline__ void add(double x) { s = __dadd_rn(s, x); }
+    __device__ __forceinline__ double value() const { return s; }
+};
+
+template <>
+struct Acc<float> {
+    float s = 0.f, c = 0.f;
+    __device__ __forceinline__ void add(float x) {
+        float y = __fsub_rn(x, c);
+        float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+/* V'(f) and V(f) (bubble.cpp:69-77). FP64: the reference's term order; FP32: Horner. */
+template <typename T>
+__device__ __forceinline__ T dV(const StepConst &k, T f) {
+    using A = Ar<T>;
+    if constexpr (std::is_same<T, double>::value) {
+        return A::add(A::sub(A::mul(k.c2, f), A::mul(k.c3, A::sq(f))), A::mul(k.c4, A::cube(f)));
+    } else {
+        return f * ((float)k.c2 + f * (-(float)k.c3 + f * (float)k.c4));
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T Vpot(const StepConst &k, T f) {
+    using A = Ar<T>;
+    if constexpr (std::is_same<T, double>::value) {
+        return A::add(A::add(A::sub(A::mul(k.v2, A::sq(f)), A::mul(k.v3, A::cube(f))), A::mul(k.v4, A::quart(f))),
+                      k.dv);
+    } else {
+        float f2 = f * f;
+        return (float)k.dv + f2 * ((float)k.v2 + f * (-(float)k.v3 + f * (float)k.v4));
+    }
+}
+
+/* Block-wide reduction of NSUM doubles into partials[block]; the last block
+ * to finish adds all partials in a fixed order and returns true with the
+ * totals in tot[] (valid in thread 0). */
+template <int NT>
+__device__ bool reduce_last_block(double (&v)[NSUM], double *partials, unsigned int *counter, double *tot) {
+    constexpr int NW = NT / 32;
+    __shared__ double red[NW][NSUM];
+    __shared__ bool is_last;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int lane = tid & 31, w = tid >> 5;
+#pragma unroll
+    for (int s = 0; s < NSUM; ++s) {
+        double x = v[s];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));
+        if (lane == 0) red[w][s] = x;
+    }
+    __syncthreads();
+    const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (tid < NSUM) {
+        double x = 0.0;
+        for (int i = 0; i < NW; ++i) x = __dadd_rn(x, red[i][tid]);
+        partials[(size_t)bid * NSUM + tid] = x;
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) is_last = (atomicAdd(counter, 1u) == nblocks - 1);
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    /* fixed-order sum: thread t takes blocks t, t+NT, ... */
+    double acc[NSUM];
+#pragma unroll
+    for (int s = 0; s < NSUM; ++s) acc[s] = 0.0;
+    for (unsigned b = tid; b < nblocks; b += NT) {
+#pragma unroll
+        for (int s = 0; s < NSUM; ++s) acc[s] = __dadd_rn(acc[s], __ldcg(partials + (size_t)b * NSUM + s));
+    }
+    __shared__ double tree[NT];
+    for (int s = 0; s < NSUM; ++s) {
+        tree[tid] = acc[s];
+        __syncthreads();
+        for (int st = NT / 2; st > 0; st >>= 1) {
+            if (tid < st) tree[tid] = __dadd_rn(tree[tid], tree[tid + st]);
+            __syncthreads();
+        }
+        if (tid == 0) tot[s] = tree[0];
+        __syncthreads();
+    }
+    if (tid == 0) *counter = 0u;
+    return true;
+}
+
+__device__ __forceinline__ int is_pow2(double x) {
+    int e;
+    double m = frexp(x, &e);
+    return (m == 0.5 || m == -0.5) ? 1 : 0;
+}
+
+/* Coefficients of the next step from the background (a, a') at its start. */
+__device__ void set_coefficients(const StepConst &k, DevState *st) {
+    const double a = st->a, ap = st->ap;
+    const int d = k.d, al = k.alpha;
+    st->fl = pow(a, (double)(d - 2 + al));
+    st->fv = pow(a, (double)(d + al));
+    st->a_kin = __dadd_rn(a, __dmul_rn(__dmul_rn(0.5, k.dt), ap));
+    st->kin_w = __dmul_rn(0.5, pow(st->a_kin, (double)(-2 * d)));
+    st->vel_w = pow(st->a_kin, (double)(-d));
+    st->adx = __dmul_rn(a, k.dx);
+    st->inv_adx = __ddiv_rn(1.0, st->adx);
+    st->adx_pow2 = is_pow2(st->adx);
+}
+
+/* The scalar part of oneStep, run by one thread of the last block:
+ * time-centred kinetic energy (bubble.cpp:838-843), a'' and the a/a'
+ * update (747-757, 860-865), H and C (873-875), pending drift (870). */
+__device__ void epilogue(const StepConst &k, DevState *st, const double *tot, bool static_bg) {
+    const double dxLD = k.dxLD, dxLD2 = __dmul_rn(k.dxLD, k.dxLD);
+    const double epot = __dmul_rn(tot[S_EP], dxLD);
+    const double egrad = __dmul_rn(tot[S_EG], dxLD);
+    const double ekhalf = __dmul_rn(tot[S_EK], dxLD);
+    const double ekprev = static_bg ? __dmul_rn(tot[S_EKIN_IN], dxLD) : st->ekin_half_prev;
+    const double ekin = __dmul_rn(0.5, __dadd_rn(ekhalf, ekprev));
+    const double etot = __dadd_rn(__dadd_rn(ekin, epot), egrad);
+    st->epot = epot;
+    st->egrad = egrad;
+    st->ekin = ekin;
+    st->etot = etot;
+    st->ekin_half_prev = ekhalf;
+    st->avphi = __dmul_rn(tot[S_PHI], dxLD);
+    st->avphip = __dmul_rn(tot[S_V], dxLD);
+    st->ekin_var = __dmul_rn(tot[Q_EK], dxLD2);
+    st->epot_var = __dmul_rn(tot[Q_EP], dxLD2);
+    st->egrad_var = __dmul_rn(tot[Q_EG], dxLD2);
+    st->etot_var = __dmul_rn(tot[Q_ET], dxLD2);
+    st->avphi_var = __dmul_rn(tot[Q_PHI], dxLD2);
+    st->avphip_var = __dmul_rn(tot[Q_V], dxLD2);
+
+    const double mpl2 = __dmul_rn(__dmul_rn(3.0, k.mpl), k.mpl);
+    double a = st->a, ap = st->ap;
+    double addot = 0.0;
+    if (k.expanding) {
+        if (k.alpha == 0)
+            addot = __ddiv_rn(__dmul_rn(-a, __dsub_rn(__dmul_rn(2.0, ekin), epot)), mpl2);
+        else
+            addot = __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(a, a), a),
+                                        __dadd_rn(__dsub_rn(__dmul_rn(2.0, epot), ekin), egrad)),
+                              mpl2);
+    }
+    const double ap_prev = ap;
+    ap = __dadd_rn(ap, __dmul_rn(k.dt, addot));
+    const double ap_atn = __ddiv_rn(__dadd_rn(ap_prev, ap), 2.0);
+    const double a_old = a;
+    a = __dadd_rn(a, __dmul_rn(k.dt, ap));
+    const double a_half = __dmul_rn(0.5, __dadd_rn(a, a_old));
+    st->H = __ddiv_rn(ap_atn, a_old);
+    st->C = k.expanding ? __dsub_rn(__dmul_rn(st->H, st->H),
+                                    __ddiv_rn(__dmul_rn(pow(a_old, (double)(2 * k.alpha)), etot), mpl2))
+                        : 0.0;
+    st->a = a;
+    st->ap = ap;
+    st->drift_p = pow(a_half, (double)(-k.d + k.alpha));
+    set_coefficients(k, st);
+}
+
+/* The step kernel. Threads (TX, TY) cover a tile of (rows, columns) =
+ * (axis d-2, axis d-1) of the lattice; for d = 3 the block marches over
+ * k.cz planes of axis 0. Loads use wrapped coordinates, so partial tiles and
+ * lattices smaller than a tile need no special case: threads outside the
+ * lattice load valid (wrapped) sites into the tile and do not store. */
+template <typename T, int D, int TX, int TY, bool DF, bool SUMS>
+__global__ void __launch_bounds__(TX *TY) k_step(StepConst k, const T *__restrict__ phi_in,
+                                                   const T *__restrict__ pi_in, T *__restrict__ phi_out,
+                                                   T *__restrict__ pi_out, T *__restrict__ loc_ek,
+                                                   T *__restrict__ loc_eg, T *__restrict__ loc_ep, DevState *st,
+                                                   double *partials) {
+    using A = Ar<T>;
+    __shared__ T tile[TY + 2][TX + 2];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int ni = k.ni, nj = k.nj, nk = k.nk;
+    const int kk = blockIdx.x * TX + tx;
+    const int jj = blockIdx.y * TY + ty;
+    const bool active = kk < nk && jj < nj;
+    const size_t sj = (size_t)nk, si = (size_t)nj * nk;
+    const size_t col = (size_t)(jj % nj) * sj + (size_t)(kk % nk);
+    const int i0 = (D == 3) ? blockIdx.z * k.cz : 0;
+    const int i1 = (D == 3) ? min(i0 + k.cz, ni) : 1;
+
+    /* background of this step (written by the previous epilogue or the host) */
+    const T fl = (T)st->fl, fv = (T)st->fv, kin_w = (T)st->kin_w, vel_w = (T)st->vel_w;
+    const T adx = (T)st->adx, inv_adx = (T)st->inv_adx;
+    const bool adx_pow2 = st->adx_pow2 != 0;
+    const T p = DF ? (T)st->drift_p : (T)1;
+    const T dt = (T)k.dt;
+    const T dx2 = (T)k.dx2, inv_dx2 = (T)k.inv_dx2;
+    const bool dx2_pow2 = k.dx2_pow2 != 0;
+    const T half = (T)0.5;
+
+    auto eff = [&](size_t idx) -> T {
+        T f = phi_in[idx];
+        if (DF) f = A::add(f, A::mul(A::mul(dt, pi_in[idx]), p));
+        return f;
+    };
+    auto grad = [&](T dphi) -> T { return adx_pow2 ? A::mul(dphi, inv_adx) : A::div(dphi, adx); };
+
+    Acc<T> acc[NSUM];
+    T prev = (T)0, next = (T)0, pinext = (T)0;
+    if (D == 3) prev = eff((size_t)((i0 - 1 + ni) % ni) * si + col);
+    T cur = eff((size_t)i0 * si + col);
+    T pic = pi_in[(size_t)i0 * si + col];
+
+    for (int i = i0; i < i1; ++i) {
+        const size_t base = (size_t)i * si;
+        if (D == 3) {
+            const int ip = (i + 1 == ni) ? 0 : i + 1;
+            const size_t nb = (size_t)ip * si + col;
+            pinext = pi_in[nb];
+            next = phi_in[nb];
+            if (DF) next = A::add(next, A::mul(A::mul(dt, pinext), p));
+        }
+        tile[ty + 1][tx + 1] = cur;
+        for (int h = ty * TX + tx; h < 2 * TX + 2 * TY; h += TX * TY) {
+            int r, c;
+            if (h < TX) { r = 0; c = h + 1; }
+            else if (h < 2 * TX) { r = TY + 1; c = h - TX + 1; }
+            else if (h < 2 * TX + TY) { r = h - 2 * TX + 1; c = 0; }
+            else { r = h - 2 * TX - TY + 1; c = TX + 1; }
+            const int gj = ((int)blockIdx.y * TY + r - 1 + nj) % nj;
+            const int gk = ((int)blockIdx.x * TX + c - 1 + nk) % nk;
+            tile[r][c] = eff(base + (size_t)gj * sj + (size_t)gk);
+        }
+        __syncthreads();
+        if (active) {
+            const T two = A::add(cur, cur);
+            /* Laplacian, axes in the reference's order 0..d-1 (bubble.cpp:731-736) */
+            T lap;
+            const T tj = A::add(A::sub(tile[ty + 2][tx + 1], two), tile[ty][tx + 1]);
+            const T tk = A::add(A::sub(tile[ty + 1][tx + 2], two), tile[ty + 1][tx]);
+            if (D == 3) lap = A::add(A::add(A::add(A::sub(next, two), prev), tj), tk);
+            else if (D == 2) lap = A::add(tj, tk);
+            else lap = tk;
+            const T flap = A::mul(fl, lap);
+            const T force = A::sub(dx2_pow2 ? A::mul(flap, inv_dx2) : A::div(flap, dx2), A::mul(fv, dV<T>(k, cur)));
+            const T pinew = A::add(pic, A::mul(dt, force));
+            const size_t o = base + col;
+            pi_out[o] = pinew;
+            phi_out[o] = DF ? cur : A::add(cur, A::mul(dt, pinew));
+            if (SUMS) {
+                /* forward gradients in the reference's naming (bubble.cpp:788-801) */
+                T gx, gy = (T)0, gz = (T)0;
+                const T dfk = A::sub(tile[ty + 1][tx + 2], cur);
+                const T dfj = A::sub(tile[ty + 2][tx + 1], cur);
+                if (D == 1) gx = grad(dfk);
+                else if (D == 2) { gx = grad(dfk); gy = grad(dfj); }
+                else { gx = grad(dfj); gy = grad(A::sub(next, cur)); gz = grad(dfk); }
+                const T eg = A::mul(half, A::add(A::add(A::sq(gx), A::sq(gy)), A::sq(gz)));
+                const T ep = Vpot<T>(k, cur);
+                const T ek = A::mul(A::mul(kin_w, pinew), pinew);
+                const T v = A::mul(pinew, vel_w);
+                const T et = A::add(A::add(ek, eg), ep);
+                acc[S_EK].add(ek);
+                acc[S_EP].add(ep);
+                acc[S_EG].add(eg);
+                acc[S_PHI].add(cur);
+                acc[S_V].add(v);
+                acc[Q_EK].add(A::sq(ek));
+                acc[Q_EP].add(A::sq(ep));
+                acc[Q_EG].add(A::sq(eg));
+                acc[Q_ET].add(A::sq(et));
+                acc[Q_PHI].add(A::sq(cur));
+                acc[Q_V].add(A::sq(v));
+                acc[S_EKIN_IN].add(A::mul(A::mul(kin_w, pic), pic));
+                if (k.want_local) {
+                    loc_ek[o] = ek;
+                    loc_eg[o] = eg;
+                    loc_ep[o] = ep;
+                }
+            }
+        }
+        __syncthreads();
+        if (D == 3) {
+            prev = cur;
+            cur = next;
+            pic = pinext;
+        }
+    }
+
+    if (SUMS) {
+        double v[NSUM];
+#pragma unroll
+        for (int s = 0; s < NSUM; ++s) v[s] = acc[s].value();
+        __shared__ double tot[NSUM];
+        if (reduce_last_block<TX * TY>(v, partials, &st->counter, tot)) {
+            if (threadIdx.x == 0 && threadIdx.y == 0) epilogue(k, st, tot, !DF);
+        }
+    }
+}
+
+/* ---- set-up kernels (once per run; plain global loads) ------------------ */
+
+__device__ __forceinline__ size_t nb_index(const StepConst &k, size_t s, int axis, int dir) {
+    size_t stride = 1;
+    for (int a = axis + 1; a < k.d; ++a) stride *= (size_t)k.n;
+    const size_t coord = (s / stride) % (size_t)k.n;
+    const size_t moved = (coord + (size_t)k.n + (size_t)(dir > 0 ? 1 : k.n - 1)) % (size_t)k.n;
+    return s - coord * stride + moved * stride;
+}
+
+template <typename T>
+__device__ __forceinline__ T load_as(const void *p, size_t i) { return static_cast<const T *>(p)[i]; }
+
+/* Initial energies with forward differences over dx (bubble.cpp:239-269) and
+ * the start of the background (271-276). */
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_ic_energies(StepConst k, size_t N, const T *__restrict__ phi,
+                                                     const T *__restrict__ pi, T *loc_ek, T *loc_eg, T *loc_ep,
+                                                     DevState *st, double *partials) {
+    double v[NSUM];
+#pragma unroll
+    for (int s = 0; s < NSUM; ++s) v[s] = 0.0;
+    const double dx = k.dx;
+    for (size_t s = blockIdx.x * (size_t)NT + threadIdx.x; s < N; s += (size_t)gridDim.x * NT) {
+        const double f = (double)phi[s];
+        double g2 = 0.0;
+        for (int ax = 0; ax < k.d; ++ax) {
+            const double g = __ddiv_rn(__dsub_rn((double)phi[nb_index(k, s, ax, +1)], f), dx);
+            g2 = __dadd_rn(g2, __dmul_rn(g, g));
+        }
+        const double eg = __dmul_rn(0.5, g2);
+        const double ep = Vpot<double>(k, f);
+        const double pv = (double)pi[s];
+        const double ek = __dmul_rn(__dmul_rn(0.5, pv), pv);
+        if (k.want_local) {
+            loc_ek[s] = (T)ek;
+            loc_eg[s] = (T)eg;
+            loc_ep[s] = (T)ep;
+        }
+        v[S_PHI] = __dadd_rn(v[S_PHI], f);
+        v[S_V] = __dadd_rn(v[S_V], pv);
+        v[S_EP] = __dadd_rn(v[S_EP], ep);
+        v[S_EG] = __dadd_rn(v[S_EG], eg);
+        v[S_EK] = __dadd_rn(v[S_EK], ek);
+    }
+    __shared__ double tot[NSUM];
+    if (reduce_last_block<NT>(v, partials, &st->counter, tot) && threadIdx.x == 0) {
+        const double dxLD = k.dxLD;
+        st->avphi = __dmul_rn(tot[S_PHI], dxLD);
+        st->avphip = __dmul_rn(tot[S_V], dxLD);
+        st->epot = __dmul_rn(tot[S_EP], dxLD);
+        st->egrad = __dmul_rn(tot[S_EG], dxLD);
+        st->ekin = __dmul_rn(tot[S_EK], dxLD);
+        st->etot = __dadd_rn(__dadd_rn(st->ekin, st->epot), st->egrad);
+        st->etot_var = st->ekin_var = st->egrad_var = st->epot_var = 0.0;
+        st->avphi_var = st->avphip_var = 0.0;
+        const double a = 1.0;
+        const double mpl2 = __dmul_rn(__dmul_rn(3.0, k.mpl), k.mpl);
+        const double H0 = k.expanding ? sqrt(__ddiv_rn(__dmul_rn(pow(a, (double)(2 * k.alpha)), st->etot), mpl2)) : 0.0;
+        double addot = 0.0;
+        if (k.expanding) {
+            if (k.alpha == 0)
+                addot = __ddiv_rn(__dmul_rn(-a, __dsub_rn(__dmul_rn(2.0, st->ekin), st->epot)), mpl2);
+            else
+                addot = __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(a, a), a),
+                                            __dadd_rn(__dsub_rn(__dmul_rn(2.0, st->epot), st->ekin), st->egrad)),
+                                  mpl2);
+        }
+        st->a = a;
+        st->ap = __dsub_rn(__dmul_rn(a, H0), __dmul_rn(__dmul_rn(0.5, k.dt), addot));
+        st->H = H0;
+        st->C = 0.0;
+        st->drift_p = 0.0;
+        set_coefficients(k, st);
+    }
+}
+
+/* Back-kick to pi_{-1/2} with the force at t = 0 and EkinHalfPrev
+ * (bubble.cpp:278-289). a = 1 here, so the force coefficients are 1. */
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_ic_backkick(StepConst k, size_t N, const T *__restrict__ phi,
+                                                     T *__restrict__ pi, DevState *st, double *partials) {
+    using A = Ar<T>;
+    double v[NSUM];
+#pragma unroll
+    for (int s = 0; s < NSUM; ++s) v[s] = 0.0;
+    const double a_mhalf = __dsub_rn(st->a, __dmul_rn(__dmul_rn(0.5, k.dt), st->ap));
+    const double w = __dmul_rn(0.5, pow(a_mhalf, (double)(-2 * k.d)));
+    const T fl = (T)pow(st->a, (double)(k.d - 2 + k.alpha)), fv = (T)pow(st->a, (double)(k.d + k.alpha));
+    const T hdt = (T)__dmul_rn(0.5, k.dt);
+    for (size_t s = blockIdx.x * (size_t)NT + threadIdx.x; s < N; s += (size_t)gridDim.x * NT) {
+        const T f = phi[s];
+        const T two = A::add(f, f);
+        T lap = (T)0;
+        for (int ax = 0; ax < k.d; ++ax) {
+            const T t = A::add(A::sub(phi[nb_index(k, s, ax, +1)], two), phi[nb_index(k, s, ax, -1)]);
+            lap = ax == 0 ? t : A::add(lap, t);
+        }
+        const T flap = A::mul(fl, lap);
+        const T force = A::sub(k.dx2_pow2 ? A::mul(flap, (T)k.inv_dx2) : A::div(flap, (T)k.dx2),
+                               A::mul(fv, dV<T>(k, f)));
+        const T pv = A::sub(pi[s], A::mul(hdt, force));
+        pi[s] = pv;
+        const double pd = (double)pv;
+        v[S_EK] = __dadd_rn(v[S_EK], __dmul_rn(__dmul_rn(w, pd), pd));
+    }
+    __shared__ double tot[NSUM];
+    if (reduce_last_block<NT>(v, partials, &st->counter, tot) && threadIdx.x == 0)
+        st->ekin_half_prev = __dmul_rn(tot[S_EK], k.dxLD);
+}
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_flush_drift(size_t N, double dt, const T *__restrict__ phi,
+                                                     const T *__restrict__ pi, T *__restrict__ out, DevState *st) {
+    using A = Ar<T>;
+    const T p = (T)st->drift_p;
+    for (size_t s = blockIdx.x * (size_t)NT + threadIdx.x; s < N; s += (size_t)gridDim.x * NT)
+        out[s] = A::add(phi[s], A::mul(A::mul((T)dt, pi[s]), p));
+}
+
+__global__ void k_clear_drift(DevState *st) { st->drift_p = 0.0; }
+
+template <typename S, typename D>
+__global__ void k_convert(const S *__restrict__ src, D *__restrict__ dst, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = (D)src[i];
+}
+
+constexpr int TX3 = 32, TY3 = 8;   /* d = 2, 3 tile: 32 columns x 8 rows */
+constexpr int TX1 = 256, TY1 = 1;  /* d = 1 tile */
+constexpr int NT_IC = 256;
+
+dim3 step_grid(const StepConst &k) {
+    if (k.d == 1) return dim3((unsigned)((k.nk + TX1 - 1) / TX1), 1, 1);
+    const unsigned gz = (k.d == 3) ? (unsigned)((k.ni + k.cz - 1) / k.cz) : 1u;
+    return dim3((unsigned)((k.nk + TX3 - 1) / TX3), (unsigned)((k.nj + TY3 - 1) / TY3), gz);
+}
+
+template <typename T, int D, bool DF, bool SUMS>
+cudaError_t launch_t(const StepConst &k, const void *phi_in, const void *pi_in, void *phi_out, void *pi_out,
+                     void *le, void *lg, void *lp, DevState *st, double *partials, cudaStream_t s) {
+    const dim3 g = step_grid(k);
+    if (D == 1) {
+        k_step<T, 1, TX1, TY1, DF, SUMS><<<g, dim3(TX1, TY1), 0, s>>>(
+            k, (const T *)phi_in, (const T *)pi_in, (T *)phi_out, (T *)pi_out, (T *)le, (T *)lg, (T *)lp, st, partials);
+    } else {
+        k_step<T, D, TX3, TY3, DF, SUMS><<<g, dim3(TX3, TY3), 0, s>>>(
+            k, (const T *)phi_in, (const T *)pi_in, (T *)phi_out, (T *)pi_out, (T *)le, (T *)lg, (T *)lp, st, partials);
+    }
+    return cudaGetLastError();
+}
+
+template <typename T, int D>
+cudaError_t launch_d(const StepConst &k, bool df, bool sums, const void *a, const void *b, void *c, void *d_,
+                     void *le, void *lg, void *lp, DevState *st, double *partials, cudaStream_t s) {
+    if (df) return launch_t<T, D, true, true>(k, a, b, c, d_, le, lg, lp, st, partials, s);
+    if (sums) return launch_t<T, D, false, true>(k, a, b, c, d_, le, lg, lp, st, partials, s);
+    return launch_t<T, D, false, false>(k, a, b, c, d_, le, lg, lp, st, partials, s);
+}
+
+template <typename T>
+cudaError_t launch_p(const StepConst &k, bool df, bool sums, const void *a, const void *b, void *c, void *d_,
+                     void *le, void *lg, void *lp, DevState *st, double *partials, cudaStream_t s) {
+    switch (k.d) {
+        case 1: return launch_d<T, 1>(k, df, sums, a, b, c, d_, le, lg, lp, st, partials, s);
+        case 2: return launch_d<T, 2>(k, df, sums, a, b, c, d_, le, lg, lp, st, partials, s);
+        case 3: return launch_d<T, 3>(k, df, sums, a, b, c, d_, le, lg, lp, st, partials, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+size_t sites(const StepConst &k) {
+    size_t N = 1;
+    for (int i = 0; i < k.d; ++i) N *= (size_t)k.n;
+    return N;
+}
+
+unsigned ic_grid(size_t N) {
+    size_t b = (N + NT_IC - 1) / NT_IC;
+    return (unsigned)(b < 148 * 8 ? (b ? b : 1) : 148 * 8);
+}
+
+}  // namespace
+
+size_t step_blocks(const StepConst &k) {
+    dim3 g = step_grid(k);
+    return (size_t)g.x * g.y * g.z;
+}
+
+size_t ic_blocks(const StepConst &k) { return ic_grid(sites(k)); }
+
+cudaError_t launch_step(int prec, const StepConst &k, bool drift_first, bool sums, const void *phi_in,
+                        const void *pi_in, void *phi_out, void *pi_out, void *loc_ek, void *loc_eg, void *loc_ep,
+                        DevState *st, double *partials, cudaStream_t s) {
+    if (prec == P_FP64)
+        return launch_p<double>(k, drift_first, sums, phi_in, pi_in, phi_out, pi_out, loc_ek, loc_eg, loc_ep, st,
+                                partials, s);
+    return launch_p<float>(k, drift_first, sums, phi_in, pi_in, phi_out, pi_out, loc_ek, loc_eg, loc_ep, st,
+                           partials, s);
+}
+
+cudaError_t launch_ic_energies(int prec, const StepConst &k, const void *phi, const void *pi, void *le, void *lg,
+                               void *lp, DevState *st, double *partials, cudaStream_t s) {
+    const size_t N = sites(k);
+    if (prec == P_FP64)
+        k_ic_energies<double, NT_IC><<<ic_grid(N), NT_IC, 0, s>>>(k, N, (const double *)phi, (const double *)pi,
+                                                                  (double *)le, (double *)lg, (double *)lp, st,
+                                                                  partials);
+    else
+        k_ic_energies<float, NT_IC><<<ic_grid(N), NT_IC, 0, s>>>(k, N, (const float *)phi, (const float *)pi,
+                                                                 (float *)le, (float *)lg, (float *)lp, st, partials);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ic_backkick(int prec, const StepConst &k, const void *phi, void *pi, DevState *st,
+                               double *partials, cudaStream_t s) {
+    const size_t N = sites(k);
+    if (prec == P_FP64)
+        k_ic_backkick<double, NT_IC><<<ic_grid(N), NT_IC, 0, s>>>(k, N, (const double *)phi, (double *)pi, st,
+                                                                  partials);
+    else
+        k_ic_backkick<float, NT_IC><<<ic_grid(N), NT_IC, 0, s>>>(k, N, (const float *)phi, (float *)pi, st,
+                                                                 partials);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_flush_drift(int prec, const StepConst &k, const void *phi, const void *pi, void *phi_out,
+                               DevState *st, cudaStream_t s) {
+    const size_t N = sites(k);
+    if (prec == P_FP64)
+        k_flush_drift<double, NT_IC><<<ic_grid(N), NT_IC, 0, s>>>(N, k.dt, (const double *)phi, (const double *)pi,
+                                                                  (double *)phi_out, st);
+    else
+        k_flush_drift<float, NT_IC><<<ic_grid(N), NT_IC, 0, s>>>(N, k.dt, (const float *)phi, (const float *)pi,
+                                                                 (float *)phi_out, st);
+    k_clear_drift<<<1, 1, 0, s>>>(st);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert(int from, int to, const void *src, void *dst, size_t n, cudaStream_t s) {
+    const unsigned g = ic_grid(n);
+    if (from == P_FP64 && to == P_FP32) k_convert<double, float><<<g, NT_IC, 0, s>>>((const double *)src, (float *)dst, n);
+    else if (from == P_FP32 && to == P_FP64) k_convert<float, double><<<g, NT_IC, 0, s>>>((const float *)src, (double *)dst, n);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+}  // namespace cb

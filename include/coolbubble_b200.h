@@ -1,0 +1,170 @@
+/* coolbubble_b200.h -- C ABI of the B200 lattice-evolution library.
+ *
+ * Drop-in for CoolBubble's evolve path (reference: Henda-M/CoolBubble). The
+ * reference has no plugin or FFI layer; its "interface" is the Bubble struct
+ * (src/bubble.hpp:34-135) driven by the time loop of src/main.cpp:274-288.
+ * Each entry point below names the reference code it replaces. Plain C types
+ * only: pointers, sizes, doubles.
+ *
+ * Conventions
+ *  - Every call returns CB_OK (0) or a negative CB_E* status; nothing exits,
+ *    aborts or throws across this ABI. cb_last_error() gives the message of
+ *    the last failed call on a handle (or of a failed cb_create*, via NULL).
+ *  - Host buffers belong to the caller; device memory belongs to the library.
+ *  - Lattice arrays are row-major with axis 0 slowest: site
+ *    s = (i0 * n + i1) * n + i2, as in src/gridfuncs.cpp:25-26.
+ *  - One CUDA stream per handle. A handle must not be used from two host
+ *    threads at once. Different handles are independent.
+ *  - Time levels follow the reference's leapfrog (src/bubble.cpp:846-876):
+ *    phi and a at whole steps, pi and a' at half steps.
+ */
+#ifndef COOLBUBBLE_B200_H
+#define COOLBUBBLE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define CB_OK 0
+#define CB_EINVAL (-1)       /* bad argument (size, pointer, parameter, CFL) */
+#define CB_ENOMEM (-2)       /* device or host allocation failed */
+#define CB_EDEVICE (-3)      /* CUDA error (message in cb_last_error) */
+#define CB_ETIMEOUT (-4)     /* a bounded wait ran out */
+#define CB_EUNSUPPORTED (-5) /* valid request this build does not handle */
+#define CB_EBUSY (-6)        /* no room now (pool admission) */
+#define CB_ENOTFOUND (-7)    /* unknown run id */
+
+/* ---- precision of the evolved fields --------------------------------- */
+#define CB_FP64 0   /* double fields and arithmetic: the parity path */
+#define CB_FP32C 1  /* float fields, compensated float per-thread sums, double cross-block
+                       sums and double Friedmann update: the speed path */
+
+/* ---- cb_step flags ---------------------------------------------------- */
+#define CB_STEP_SUMS 1   /* measure the box averages in the last step (bubble.cpp:761-844) */
+#define CB_STEP_LOCAL 2  /* store the local Ekin/gradphi/potEnergy arrays in the last step
+                            (bubble.cpp:827-833; needs memorysave == 0) */
+
+/* Run parameters. In the reference these are main.cpp globals (main.cpp:45-50)
+ * and def.h macros (def.h:29-76); here they are per run. */
+typedef struct cb_params {
+    int d;            /* 1, 2 or 3 (main.cpp:135) */
+    int n_grids;      /* points per axis, >= 2 */
+    double L;         /* box size; dx = L / n_grids (bubble.hpp:45) */
+    double c;         /* potential parameter (bubble.cpp:69-77) */
+    double dt;        /* TIME_STEP (def.h:33); must satisfy dt < dx / sqrt(d) (main.cpp:171-183) */
+    int alpha;        /* ALPHAVAL (def.h:57): 0 cosmic time, 1 conformal time */
+    int expansion;    /* def.h:56; the background expands only if expansion != 0 and d == 3 (bubble.hpp:77) */
+    double mpl;       /* Mpl (def.h:58) */
+    double delta_v;   /* DeltaV, 1 in the reference (bubble.cpp:161) */
+    int precision;    /* CB_FP64 or CB_FP32C */
+    int memorysave;   /* def.h:64: 0 keeps local energy arrays for snapshots */
+} cb_params;
+
+/* State handed to the time loop by the reference constructor
+ * (bubble.cpp:271-291): a_0, a'_{-1/2}, H_0 and the kinetic energy at t = -1/2. */
+typedef struct cb_scalars {
+    double t;
+    double a;
+    double ap;
+    double H;
+    double ekin_half_prev;
+} cb_scalars;
+
+/* One line of EnergyDensities.dat (bubble.cpp:977-989) plus the leapfrog
+ * scalars. The *_var entries are the raw sums of squares (the reference's
+ * static *Var variables, bubble.cpp:44); the file prints their square roots. */
+typedef struct cb_sums {
+    double t, a, H, C;
+    double etot, ekin, egrad, epot;
+    double etot_var, ekin_var, egrad_var, epot_var;
+    double avphi, avphi_var, avphip, avphip_var;
+    double ap, ekin_half_prev;
+} cb_sums;
+
+typedef struct cb_handle cb_handle;
+
+/* Upload the state the reference's Bubble constructor leaves behind
+ * (phi_0, pi_{-1/2}, scalars) and take over its time loop. Replaces the
+ * reference's ownership of phi/pi/dpi (bubble.hpp:69, bubble.cpp:173-182).
+ * phi, pi: n_grids^d doubles (host). */
+int cb_create(const cb_params *p, const double *phi, const double *pi_mhalf, const cb_scalars *s0,
+              cb_handle **out);
+
+/* Upload a raw initial condition (phi_0, pi_0 at t = 0; pi0 may be NULL for
+ * pi = 0) and run the constructor's set-up on the device: initial energies,
+ * H_0, a'_{-1/2}, back-kick to pi_{-1/2} and EkinHalfPrev (bubble.cpp:236-291).
+ * `initial` (may be NULL) receives the t = 0 line of EnergyDensities.dat. */
+int cb_create_from_ic(const cb_params *p, const double *phi0, const double *pi0, cb_sums *initial,
+                      cb_handle **out);
+
+/* Advance nsteps leapfrog steps: nsteps calls of Bubble::oneStep
+ * (bubble.cpp:849-876) including computeForces (716-743), measureEnergies
+ * (761-844), addot (747-757) and the periodic neighbours of gridfuncs.cpp:31-51.
+ * flags: CB_STEP_SUMS / CB_STEP_LOCAL apply to the last of the nsteps steps;
+ * `out` (may be NULL) receives that step's line. An expanding background
+ * measures the sums every step regardless (the Friedmann update needs them). */
+int cb_step(cb_handle *h, int nsteps, int flags, cb_sums *out);
+
+/* cb_step without sums, bracketed by CUDA events on the run's stream;
+ * waits for the steps and returns their device time in milliseconds. */
+int cb_step_timed(cb_handle *h, int nsteps, int flags, double *device_ms);
+
+/* Wait for all work queued on the run's stream; reports deferred CUDA errors. */
+int cb_sync(cb_handle *h);
+
+/* CUDA events on the run's stream: cb_timer_start records the start,
+ * cb_timer_stop records the end, waits for it and returns the device time
+ * in milliseconds between the two. */
+int cb_timer_start(cb_handle *h);
+int cb_timer_stop(cb_handle *h, double *device_ms);
+
+/* Select the CUDA device for the runs this host thread creates next
+ * (one process per GPU: call it with the local rank). */
+int cb_set_device(int device);
+
+/* Page-locked host buffers (faster uploads and downloads); NULL on failure. */
+void *cb_pinned_alloc(size_t bytes);
+int cb_pinned_free(void *p);
+
+/* The latest scalars (t, a, a', H, C and the last measured sums). */
+int cb_get_sums(cb_handle *h, cb_sums *out);
+
+/* Download phi (whole step), pi (half step) and the local energy arrays
+ * stored by the last CB_STEP_LOCAL step (or by the set-up). Any pointer may
+ * be NULL. Replaces reading Bubble::phi/pi/Ekin/gradphi/potEnergy
+ * (bubble.cpp:898-917). */
+int cb_get_fields(cb_handle *h, double *phi, double *pi, double *ekin, double *egrad, double *epot);
+
+/* Same, converted to float on the device first (the snapshot stores float,
+ * bubble.cpp:905-915), halving the bytes moved. */
+int cb_get_fields_f32(cb_handle *h, float *phi, float *pi, float *ekin, float *egrad, float *epot);
+
+/* Number of |k| shells: floor(sqrt(d) * n / 2) + 1 (bubble.hpp:49, bubble.cpp:671). */
+int cb_nbins(int d, int n_grids);
+
+/* Power spectrum of the current phi: a d-dimensional real-to-complex DFT with
+ * shell binning, replacing FourierTransform + ComputePowerSpectrum
+ * (bubble.cpp:642-709). power[b] = sum over the modes of shell b of
+ * w * pref * k^d * Pnorm * |phi_k|^2, weight[b] = sum w, ksum[b] = sum w * k.
+ * The file line of shell b is ksum/weight, ksum/weight/a, power/weight. */
+int cb_power_spectrum(cb_handle *h, double *power, double *weight, double *ksum, int nbins);
+
+/* Release the handle and its device memory. */
+int cb_destroy(cb_handle *h);
+
+/* Message of the last failed call on h (NULL: of the last failed create). */
+const char *cb_last_error(const cb_handle *h);
+const char *cb_status_string(int status);
+
+/* Device bytes a run of these parameters holds (admission budgeting). */
+int64_t cb_footprint_bytes(const cb_params *p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* COOLBUBBLE_B200_H */

@@ -1,0 +1,200 @@
+"""GPU parity of the fused step kernels against the reference (golden
+fixtures) and the CPU restatement (oracle), through the C ABI.
+
+Bars (stated here, applied below):
+  FP64 fields: max|gpu - ref| / max(max|ref|, 1e-300) <= 1e-12 over the run
+  FP64 box averages and a, a', H: relative 1e-10 (C on the scale of H^2;
+      signed sums <phi>, <phi'> on the scale sqrt(N * sum x^2) >= sum |x|)
+  FP32C box averages: relative 1e-5 of the FP64 oracle (Etot scale for the
+      kinetic energy, which starts near 0 for bubbles)
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, load_golden
+from ic_helpers import bubbles, smooth_noise
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-12
+SUM_TOL = 1e-10
+SUM_KEYS = {"etot": "Etot", "ekin": "Ekintot", "egrad": "Egradtot", "epot": "Epottot", "a": "a", "ap": "ap",
+            "H": "H", "ekin_half_prev": "EkinHalfPrev", "etot_var": "EtotVar", "ekin_var": "EkintotVar",
+            "egrad_var": "EgradtotVar", "epot_var": "EpottotVar", "avphi_var": "avphiVar",
+            "avphip_var": "avphiPVar"}
+
+
+def field_err(a, ref):
+    return float(np.abs(a - ref).max() / max(np.abs(ref).max(), 1e-300))
+
+
+def check_sums(got, ref, N, tol=SUM_TOL, where=""):
+    """got: cb_sums dict; ref: oracle/reference scalars dict (18 names)."""
+    for k, rk in SUM_KEYS.items():
+        r = ref[rk]
+        assert abs(got[k] - r) <= tol * max(abs(r), 1e-300), (where, k, got[k], r)
+    for k, rk in (("avphi", "avphi"), ("avphip", "avphiP")):
+        scale = np.sqrt(N * ref[rk + "Var"]) if ref[rk + "Var"] > 0 else abs(ref[rk])
+        assert abs(got[k] - ref[rk]) <= tol * max(scale, 1e-300), (where, k, got[k], ref[rk])
+    assert abs(got["C"] - ref["C"]) <= tol * max(ref["H"] ** 2, 1e-300), (where, "C", got["C"], ref["C"])
+
+
+def params_from(meta, precision="fp64", memorysave=0):
+    import coolbubble_b200 as cb
+    return cb.make_params(meta["d"], meta["n"], meta["L"], meta["c"], meta["dt"], alpha=meta.get("alpha", 0),
+                          expansion=meta.get("expansion", 0), mpl=meta.get("mpl", 200.0), precision=precision,
+                          memorysave=memorysave)
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_fp64_matches_reference_golden(name):
+    import coolbubble_b200 as cb
+    from oracle.bridge import SCALAR_NAMES
+    g = load_golden(name)
+    m = g["meta"]
+    s = cb.Bubble(params_from(m), g["phi0"], g["pi0"])
+    f = s.fields()
+    # set-up on the device (bubble.cpp:236-291)
+    assert field_err(f["phi"], g["phi_start"]) == 0.0
+    assert field_err(f["pi"], g["pi_start"]) <= FIELD_TOL
+    for k in ("ekin", "egrad", "epot"):
+        assert field_err(f[k], g[k + "_start"]) <= FIELD_TOL, k
+    ref0 = dict(zip(SCALAR_NAMES, g["scalars"][0]))
+    for k, rk in (("etot", "Etot"), ("ekin", "Ekintot"), ("egrad", "Egradtot"), ("epot", "Epottot"), ("a", "a"),
+                  ("ap", "ap"), ("H", "H"), ("ekin_half_prev", "EkinHalfPrev")):
+        assert s.last[k] == pytest.approx(ref0[rk], rel=SUM_TOL, abs=1e-300), k
+    N = m["n"] ** m["d"]
+    for it in range(1, m["steps"] + 1):
+        got = s.step(1, sums=True, local=(it == m["steps"]))
+        ref = dict(zip(SCALAR_NAMES, g["scalars"][it]))
+        check_sums(got, ref, N, where=(name, it))
+        assert got["t"] == ref["t"]
+    f = s.fields()
+    for k in ("phi", "pi", "ekin", "egrad", "epot"):
+        assert field_err(f[k], g[k + "_end"]) <= FIELD_TOL, (k, field_err(f[k], g[k + "_end"]))
+
+
+@pytest.mark.parametrize("name", ["d2_bubbles", "d3_expanding", "d3_thermal"])
+def test_dropin_create_from_reference_state(name):
+    """cb_create takes the state the reference constructor leaves behind."""
+    import coolbubble_b200 as cb
+    from oracle.bridge import SCALAR_NAMES
+    g = load_golden(name)
+    m = g["meta"]
+    sc0 = dict(zip(SCALAR_NAMES, g["scalars"][0]))
+    state = (g["phi_start"], g["pi_start"], dict(t=0.0, a=sc0["a"], ap=sc0["ap"], H=sc0["H"],
+                                                  ekin_half_prev=sc0["EkinHalfPrev"]))
+    s = cb.Bubble(params_from(m), state=state)
+    got = s.step(m["steps"], sums=True, local=True)
+    check_sums(got, dict(zip(SCALAR_NAMES, g["scalars"][-1])), m["n"] ** m["d"], where=name)
+    f = s.fields()
+    for k in ("phi", "pi", "ekin", "egrad", "epot"):
+        assert field_err(f[k], g[k + "_end"]) <= FIELD_TOL, k
+
+
+def test_chunked_steps_equal_single_steps_bitwise():
+    import coolbubble_b200 as cb
+    g = load_golden("d2_bubbles")
+    p = params_from(g["meta"])
+    a = cb.Bubble(p, g["phi0"], g["pi0"])
+    b = cb.Bubble(p, g["phi0"], g["pi0"])
+    sa = a.step(40, sums=True, local=True)
+    for _ in range(39):
+        b.step(1, sums=False)
+    sb = b.step(1, sums=True, local=True)
+    assert sa == sb
+    fa, fb = a.fields(), b.fields()
+    for k in fa:
+        np.testing.assert_array_equal(fa[k], fb[k])
+
+
+def _oracle_run(d, n, L, c, dt, phi0, pi0, steps, every, **kw):
+    from oracle import bridge as B
+    o = B.Oracle(d, n, L, c, dt, phi0, pi0, **kw)
+    out = []
+    done = 0
+    while done < steps:
+        o.step(every)
+        done += every
+        out.append(o.scalars())
+    return o, out
+
+
+@pytest.mark.parametrize("case", [
+    # C1 shape: d = 2, N = 512, L = 32, c = 4, 5 bubbles, static, dt = 0.1 dx
+    dict(d=2, n=512, L=32.0, c=4.0, steps=100, every=20, ic="bubbles", nb=5),
+    # C2 shape at reduced N: d = 3 expanding, Mpl = 10, 8 bubbles with the 1.3 radius
+    dict(d=3, n=64, L=16.0, c=4.0, steps=100, every=20, ic="bubbles", nb=8, expansion=1, mpl=10.0),
+    # partial tiles (96 is not a multiple of 32 along the march chunk), static smooth field
+    dict(d=3, n=40, L=20.0, c=2.0, steps=60, every=20, ic="noise"),
+    # d = 1, long line
+    dict(d=1, n=4096, L=64.0, c=4.0, steps=100, every=25, ic="noise"),
+    # dx^2 not a power of two: the exact-division path
+    dict(d=2, n=96, L=30.0, c=5.0, steps=80, every=20, ic="bubbles", nb=4),
+])
+def test_fp64_matches_oracle(case):
+    import coolbubble_b200 as cb
+    d, n, L, c = case["d"], case["n"], case["L"], case["c"]
+    dt = 0.1 * L / n
+    if case["ic"] == "bubbles":
+        phi0, pi0 = bubbles(d, n, L, c, case["nb"], seed=7), None
+    else:
+        phi0 = smooth_noise(d, n, 0.3, seed=3)
+        pi0 = smooth_noise(d, n, 0.05, seed=4)
+    kw = dict(expansion=case.get("expansion", 0), mpl=case.get("mpl", 200.0))
+    o, ref = _oracle_run(d, n, L, c, dt, phi0, pi0, case["steps"], case["every"], **kw)
+    s = cb.Bubble(cb.make_params(d, n, L, c, dt, **kw), phi0, pi0)
+    for r in ref:
+        got = s.step(case["every"], sums=True, local=True)
+        check_sums(got, r, n ** d, where=case)
+    f, fo = s.fields(), o.fields()
+    for k in ("phi", "pi", "ekin", "egrad", "epot"):
+        assert field_err(f[k], fo[k]) <= FIELD_TOL, (k, field_err(f[k], fo[k]))
+
+
+@pytest.mark.parametrize("case", [
+    dict(d=3, n=64, L=16.0, c=4.0, steps=100, ic="bubbles", nb=8, expansion=1, mpl=10.0),
+    dict(d=3, n=128, L=32.0, c=2.0, steps=100, ic="noise"),
+    dict(d=2, n=256, L=32.0, c=4.0, steps=200, ic="bubbles", nb=5),
+])
+def test_fp32c_energies_within_1e5_of_fp64_oracle(case):
+    import coolbubble_b200 as cb
+    d, n, L, c = case["d"], case["n"], case["L"], case["c"]
+    dt = 0.1 * L / n
+    if case["ic"] == "bubbles":
+        phi0, pi0 = bubbles(d, n, L, c, case["nb"], seed=11), None
+    else:
+        phi0, pi0 = smooth_noise(d, n, 0.3, seed=5), smooth_noise(d, n, 0.05, seed=6)
+    kw = dict(expansion=case.get("expansion", 0), mpl=case.get("mpl", 200.0))
+    o, ref = _oracle_run(d, n, L, c, dt, phi0, pi0, case["steps"], case["steps"], **kw)
+    s = cb.Bubble(cb.make_params(d, n, L, c, dt, precision="fp32c", **kw), phi0, pi0)
+    got = s.step(case["steps"], sums=True)
+    r = ref[-1]
+    etot = abs(r["Etot"])
+    for k, rk in (("etot", "Etot"), ("egrad", "Egradtot"), ("epot", "Epottot")):
+        assert abs(got[k] - r[rk]) <= 1e-5 * abs(r[rk]), (k, got[k], r[rk])
+    assert abs(got["ekin"] - r["Ekintot"]) <= 1e-5 * etot
+    assert abs(got["a"] - r["a"]) <= 1e-10 * abs(r["a"])
+
+
+def test_runs_are_deterministic():
+    import coolbubble_b200 as cb
+    d, n, L, c = 3, 48, 12.0, 4.0
+    phi0 = bubbles(d, n, L, c, 6, seed=2)
+    p = cb.make_params(d, n, L, c, 0.1 * L / n, expansion=1, mpl=10.0)
+    runs = []
+    for _ in range(2):
+        s = cb.Bubble(p, phi0)
+        runs.append((s.step(30, sums=True), s.fields()["phi"]))
+    assert runs[0][0] == runs[1][0]
+    np.testing.assert_array_equal(runs[0][1], runs[1][1])
+
+
+def test_f32_download_is_rounded_fp64_state():
+    import coolbubble_b200 as cb
+    g = load_golden("d3_thermal")
+    s = cb.Bubble(params_from(g["meta"]), g["phi0"], g["pi0"])
+    s.step(10, sums=True, local=True)
+    f64, f32 = s.fields(), s.fields_f32()
+    for k in f64:
+        np.testing.assert_array_equal(f32[k], f64[k].astype(np.float32))
