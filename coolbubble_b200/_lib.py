@@ -68,10 +68,12 @@ _SIGS = {
     "cb_pinned_alloc": (C.c_void_p, [C.c_size_t]),
     "cb_pinned_free": (C.c_int, [C.c_void_p]),
     "cb_get_sums": (C.c_int, [_h, C.POINTER(cb_sums)]),
+    "cb_device_error": (C.c_int, [_h, C.POINTER(C.c_int)]),
     "cb_get_fields": (C.c_int, [_h, _dp, _dp, _dp, _dp, _dp]),
     "cb_get_fields_f32": (C.c_int, [_h, _fp, _fp, _fp, _fp, _fp]),
     "cb_nbins": (C.c_int, [C.c_int, C.c_int]),
     "cb_power_spectrum": (C.c_int, [_h, _dp, _dp, _dp, C.c_int]),
+    "cb_dft_r2c": (C.c_int, [C.c_int, C.c_int, _dp, _dp]),
     "cb_destroy": (C.c_int, [_h]),
     "cb_last_error": (C.c_char_p, [_h]),
     "cb_status_string": (C.c_char_p, [C.c_int]),

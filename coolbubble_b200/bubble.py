@@ -92,6 +92,11 @@ class Bubble:
     def sync(self):
         check(L.lib.cb_sync(self._h), self._h)
 
+    def device_error(self):
+        code = L.C.c_int()
+        check(L.lib.cb_device_error(self._h, L.C.byref(code)), self._h)
+        return code.value
+
     def sums(self):
         s = L.cb_sums()
         check(L.lib.cb_get_sums(self._h, L.C.byref(s)), self._h)

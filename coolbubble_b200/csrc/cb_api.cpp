@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -110,6 +111,8 @@ StepConst make_const(const cb_params *p) {
     k.alpha = p->alpha;
     k.expanding = (p->expansion != 0 && p->d == 3) ? 1 : 0;
     k.want_local = 0;
+    const char *path = std::getenv("CB_STEP_PATH");
+    k.force_generic = (path && std::string(path) == "generic") ? 1 : 0;
     return k;
 }
 
@@ -133,10 +136,21 @@ int sync(cb_handle *h, const char *what) {
     return CB_OK;
 }
 
-int read_state(cb_handle *h, DevState &s) {
+int read_state_raw(cb_handle *h, DevState &s) {
     cudaError_t e = cudaMemcpyAsync(&s, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "reading device state");
     return sync(h, "reading device state");
+}
+
+int read_state(cb_handle *h, DevState &s) {
+    int r = read_state_raw(h, s);
+    if (r != CB_OK) return r;
+    if (s.err != 0) {
+        char b[128];
+        std::snprintf(b, sizeof b, "a bounded device wait ran out (error word 0x%x); the step did not complete", s.err);
+        return fail(h, CB_ETIMEOUT, b);
+    }
+    return CB_OK;
 }
 
 void fill_sums(const cb_handle *h, const DevState &s, cb_sums *o) {
@@ -474,6 +488,15 @@ int cb_pinned_free(void *p) {
 int cb_sync(cb_handle *h) {
     if (!h) return fail(nullptr, CB_EINVAL, "handle is NULL");
     return sync(h, "synchronising the run's stream");
+}
+
+int cb_device_error(cb_handle *h, int *code) {
+    if (!h || !code) return fail(h, CB_EINVAL, "handle and code must not be NULL");
+    DevState s;
+    int r = read_state_raw(h, s);
+    if (r != CB_OK) return r;
+    *code = s.err;
+    return CB_OK;
 }
 
 int cb_get_sums(cb_handle *h, cb_sums *out) {

@@ -66,6 +66,7 @@ struct StepConst {
     double dxLD, mpl;
     int alpha, expanding;
     int want_local;
+    int force_generic;  /* 1: always use the generic tile kernel (diagnostics and cross-checks) */
 };
 
 /* Kernel launchers (cb_step.cu). Each returns the cudaError_t of the launch. */
@@ -74,8 +75,14 @@ enum Prec { P_FP64 = 0, P_FP32 = 1 };
 cudaError_t launch_step(int prec, const StepConst &k, bool drift_first, bool sums, const void *phi_in,
                         const void *pi_in, void *phi_out, void *pi_out, void *loc_ek, void *loc_eg, void *loc_ep,
                         DevState *st, double *partials, cudaStream_t s);
-/* Number of blocks (and so of partial-sum slots) a step launch uses. */
+/* Number of blocks (and so of partial-sum slots) a step launch may use. */
 size_t step_blocks(const StepConst &k);
+
+/* d = 3 kernel with TMA-staged row tiles (cb_step3.cu). */
+bool step3_geometry(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid);
+cudaError_t launch_step3(int prec, const StepConst &k, bool drift_first, bool sums, const void *phi_in,
+                         const void *pi_in, void *phi_out, void *pi_out, void *loc_ek, void *loc_eg, void *loc_ep,
+                         DevState *st, double *partials, cudaStream_t s);
 
 cudaError_t launch_ic_energies(int prec, const StepConst &k, const void *phi, const void *pi, void *loc_ek,
                                void *loc_eg, void *loc_ep, DevState *st, double *partials, cudaStream_t s);

@@ -1,0 +1,226 @@
+/* cb_step_common.cuh -- device code shared by the step kernels: explicitly
+ * rounded FP64 arithmetic in the reference's evaluation order, per-thread
+ * accumulators, the potential, the deterministic last-block reduction and
+ * the scalar epilogue of a step (reference src/bubble.cpp:747-876). */
+#ifndef CB_STEP_COMMON_CUH
+#define CB_STEP_COMMON_CUH
+
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "cb_internal.h"
+
+namespace cb {
+namespace {
+
+template <typename T>
+struct Ar;
+
+template <>
+struct Ar<double> {
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    static __device__ __forceinline__ double sq(double x) { return __dmul_rn(x, x); }
+    /* x^3 and x^4 from the exact square p + e (Dekker's two-product through an fma), rounded once */
+    static __device__ __forceinline__ double cube(double x) {
+        double p = __dmul_rn(x, x);
+        double e = __fma_rn(x, x, -p);
+        return __fma_rn(p, x, __dmul_rn(e, x));
+    }
+    static __device__ __forceinline__ double quart(double x) {
+        double p = __dmul_rn(x, x);
+        double e = __fma_rn(x, x, -p);
+        return __fma_rn(p, p, __dmul_rn(__dadd_rn(p, p), e));
+    }
+};
+
+template <>
+struct Ar<float> {
+    static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
+    static __device__ __forceinline__ float add(float a, float b) { return a + b; }
+    static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
+    static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+    static __device__ __forceinline__ float sq(float x) { return x * x; }
+    static __device__ __forceinline__ float cube(float x) { return x * x * x; }
+    static __device__ __forceinline__ float quart(float x) { float p = x * x; return p * p; }
+};
+
+/* Per-thread accumulator: double for FP64, Kahan-compensated float for FP32C. */
+template <typename T>
+struct Acc;
+
+template <>
+struct Acc<double> {
+    double s = 0.0;
+    __device__ __forceinline__ void add(double x) { s = __dadd_rn(s, x); }
+    __device__ __forceinline__ double value() const { return s; }
+};
+
+template <>
+struct Acc<float> {
+    float s = 0.f, c = 0.f;
+    __device__ __forceinline__ void add(float x) {
+        float y = __fsub_rn(x, c);
+        float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+/* V'(f) and V(f) (bubble.cpp:69-77). FP64: the reference's term order; FP32: Horner. */
+template <typename T>
+__device__ __forceinline__ T dV(const StepConst &k, T f) {
+    using A = Ar<T>;
+    if constexpr (std::is_same<T, double>::value) {
+        return A::add(A::sub(A::mul(k.c2, f), A::mul(k.c3, A::sq(f))), A::mul(k.c4, A::cube(f)));
+    } else {
+        return f * ((float)k.c2 + f * (-(float)k.c3 + f * (float)k.c4));
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T Vpot(const StepConst &k, T f) {
+    using A = Ar<T>;
+    if constexpr (std::is_same<T, double>::value) {
+        return A::add(A::add(A::sub(A::mul(k.v2, A::sq(f)), A::mul(k.v3, A::cube(f))), A::mul(k.v4, A::quart(f))),
+                      k.dv);
+    } else {
+        float f2 = f * f;
+        return (float)k.dv + f2 * ((float)k.v2 + f * (-(float)k.v3 + f * (float)k.v4));
+    }
+}
+
+/* Block-wide reduction of NSUM doubles into partials[block]; the last block
+ * to finish adds all partials in a fixed order and returns true with the
+ * totals in tot[] (valid in thread 0). */
+template <int NT>
+__device__ bool reduce_last_block(double (&v)[NSUM], double *partials, unsigned int *counter, double *tot) {
+    constexpr int NW = NT / 32;
+    __shared__ double red[NW][NSUM];
+    __shared__ bool is_last;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int lane = tid & 31, w = tid >> 5;
+#pragma unroll
+    for (int s = 0; s < NSUM; ++s) {
+        double x = v[s];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));
+        if (lane == 0) red[w][s] = x;
+    }
+    __syncthreads();
+    const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (tid < NSUM) {
+        double x = 0.0;
+        for (int i = 0; i < NW; ++i) x = __dadd_rn(x, red[i][tid]);
+        partials[(size_t)bid * NSUM + tid] = x;
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) is_last = (atomicAdd(counter, 1u) == nblocks - 1);
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    /* fixed-order sum: thread t takes blocks t, t+NT, ... */
+    double acc[NSUM];
+#pragma unroll
+    for (int s = 0; s < NSUM; ++s) acc[s] = 0.0;
+    for (unsigned b = tid; b < nblocks; b += NT) {
+#pragma unroll
+        for (int s = 0; s < NSUM; ++s) acc[s] = __dadd_rn(acc[s], __ldcg(partials + (size_t)b * NSUM + s));
+    }
+    __shared__ double tree[NT];
+    for (int s = 0; s < NSUM; ++s) {
+        tree[tid] = acc[s];
+        __syncthreads();
+        for (int st = NT / 2; st > 0; st >>= 1) {
+            if (tid < st) tree[tid] = __dadd_rn(tree[tid], tree[tid + st]);
+            __syncthreads();
+        }
+        if (tid == 0) tot[s] = tree[0];
+        __syncthreads();
+    }
+    if (tid == 0) *counter = 0u;
+    return true;
+}
+
+__device__ __forceinline__ int is_pow2(double x) {
+    int e;
+    double m = frexp(x, &e);
+    return (m == 0.5 || m == -0.5) ? 1 : 0;
+}
+
+/* Coefficients of the next step from the background (a, a') at its start. */
+__device__ void set_coefficients(const StepConst &k, DevState *st) {
+    const double a = st->a, ap = st->ap;
+    const int d = k.d, al = k.alpha;
+    st->fl = pow(a, (double)(d - 2 + al));
+    st->fv = pow(a, (double)(d + al));
+    st->a_kin = __dadd_rn(a, __dmul_rn(__dmul_rn(0.5, k.dt), ap));
+    st->kin_w = __dmul_rn(0.5, pow(st->a_kin, (double)(-2 * d)));
+    st->vel_w = pow(st->a_kin, (double)(-d));
+    st->adx = __dmul_rn(a, k.dx);
+    st->inv_adx = __ddiv_rn(1.0, st->adx);
+    st->adx_pow2 = is_pow2(st->adx);
+}
+
+/* The scalar part of oneStep, run by one thread of the last block:
+ * time-centred kinetic energy (bubble.cpp:838-843), a'' and the a/a'
+ * update (747-757, 860-865), H and C (873-875), pending drift (870). */
+__device__ void epilogue(const StepConst &k, DevState *st, const double *tot, bool static_bg) {
+    const double dxLD = k.dxLD, dxLD2 = __dmul_rn(k.dxLD, k.dxLD);
+    const double epot = __dmul_rn(tot[S_EP], dxLD);
+    const double egrad = __dmul_rn(tot[S_EG], dxLD);
+    const double ekhalf = __dmul_rn(tot[S_EK], dxLD);
+    const double ekprev = static_bg ? __dmul_rn(tot[S_EKIN_IN], dxLD) : st->ekin_half_prev;
+    const double ekin = __dmul_rn(0.5, __dadd_rn(ekhalf, ekprev));
+    const double etot = __dadd_rn(__dadd_rn(ekin, epot), egrad);
+    st->epot = epot;
+    st->egrad = egrad;
+    st->ekin = ekin;
+    st->etot = etot;
+    st->ekin_half_prev = ekhalf;
+    st->avphi = __dmul_rn(tot[S_PHI], dxLD);
+    st->avphip = __dmul_rn(tot[S_V], dxLD);
+    st->ekin_var = __dmul_rn(tot[Q_EK], dxLD2);
+    st->epot_var = __dmul_rn(tot[Q_EP], dxLD2);
+    st->egrad_var = __dmul_rn(tot[Q_EG], dxLD2);
+    st->etot_var = __dmul_rn(tot[Q_ET], dxLD2);
+    st->avphi_var = __dmul_rn(tot[Q_PHI], dxLD2);
+    st->avphip_var = __dmul_rn(tot[Q_V], dxLD2);
+
+    const double mpl2 = __dmul_rn(__dmul_rn(3.0, k.mpl), k.mpl);
+    double a = st->a, ap = st->ap;
+    double addot = 0.0;
+    if (k.expanding) {
+        if (k.alpha == 0)
+            addot = __ddiv_rn(__dmul_rn(-a, __dsub_rn(__dmul_rn(2.0, ekin), epot)), mpl2);
+        else
+            addot = __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(a, a), a),
+                                        __dadd_rn(__dsub_rn(__dmul_rn(2.0, epot), ekin), egrad)),
+                              mpl2);
+    }
+    const double ap_prev = ap;
+    ap = __dadd_rn(ap, __dmul_rn(k.dt, addot));
+    const double ap_atn = __ddiv_rn(__dadd_rn(ap_prev, ap), 2.0);
+    const double a_old = a;
+    a = __dadd_rn(a, __dmul_rn(k.dt, ap));
+    const double a_half = __dmul_rn(0.5, __dadd_rn(a, a_old));
+    st->H = __ddiv_rn(ap_atn, a_old);
+    st->C = k.expanding ? __dsub_rn(__dmul_rn(st->H, st->H),
+                                    __ddiv_rn(__dmul_rn(pow(a_old, (double)(2 * k.alpha)), etot), mpl2))
+                        : 0.0;
+    st->a = a;
+    st->ap = ap;
+    st->drift_p = pow(a_half, (double)(-k.d + k.alpha));
+    set_coefficients(k, st);
+}
+
+}  // namespace
+}  // namespace cb
+
+#endif

@@ -130,6 +130,11 @@ int cb_set_device(int device);
 void *cb_pinned_alloc(size_t bytes);
 int cb_pinned_free(void *p);
 
+/* The run's device error word: 0, or the code a kernel recorded when one of
+ * its bounded waits ran out (the kernel then returned without finishing the
+ * step; calls that read the device state report CB_ETIMEOUT). */
+int cb_device_error(cb_handle *h, int *code);
+
 /* The latest scalars (t, a, a', H, C and the last measured sums). */
 int cb_get_sums(cb_handle *h, cb_sums *out);
 
@@ -152,6 +157,12 @@ int cb_nbins(int d, int n_grids);
  * w * pref * k^d * Pnorm * |phi_k|^2, weight[b] = sum w, ksum[b] = sum w * k.
  * The file line of shell b is ksum/weight, ksum/weight/a, power/weight. */
 int cb_power_spectrum(cb_handle *h, double *power, double *weight, double *ksum, int nbins);
+
+/* The d-dimensional real-to-complex DFT alone (host in, host out), in
+ * FFTW's r2c layout as the reference's fftw_plan_dft_r2c produces it
+ * (bubble.cpp:648-651): out holds n^(d-1) * (n/2+1) complex values as
+ * interleaved (re, im) doubles. n_grids up to 6144 with prime factors <= 13. */
+int cb_dft_r2c(int d, int n_grids, const double *in, double *out);
 
 /* Release the handle and its device memory. */
 int cb_destroy(cb_handle *h);

@@ -198,3 +198,54 @@ def test_f32_download_is_rounded_fp64_state():
     f64, f32 = s.fields(), s.fields_f32()
     for k in f64:
         np.testing.assert_array_equal(f32[k], f64[k].astype(np.float32))
+
+
+@pytest.mark.parametrize("case", [
+    dict(d=3, n=64, L=16.0, c=4.0, expansion=1, mpl=10.0, prec="fp64"),
+    dict(d=3, n=128, L=32.0, c=2.0, expansion=0, mpl=200.0, prec="fp64"),
+    dict(d=3, n=96, L=24.0, c=3.0, expansion=0, mpl=200.0, prec="fp64"),
+])
+def test_tiled_kernel_equals_generic_kernel_fp64(case, monkeypatch):
+    """The TMA-tiled d = 3 kernel does the generic kernel's arithmetic op for op."""
+    import coolbubble_b200 as cb
+    d, n, L, c = case["d"], case["n"], case["L"], case["c"]
+    p = cb.make_params(d, n, L, c, 0.1 * L / n, expansion=case["expansion"], mpl=case["mpl"], precision=case["prec"])
+    phi0 = bubbles(d, n, L, c, 6, seed=4)
+    pi0 = smooth_noise(d, n, 0.02, seed=5)
+    tiled = cb.Bubble(p, phi0, pi0)
+    monkeypatch.setenv("CB_STEP_PATH", "generic")
+    generic = cb.Bubble(p, phi0, pi0)
+    monkeypatch.delenv("CB_STEP_PATH")
+    a = tiled.step(25, sums=True, local=True)
+    b = generic.step(25, sums=True, local=True)
+    for key in a:
+        assert a[key] == b[key], key
+    fa, fb = tiled.fields(), generic.fields()
+    for key in fa:
+        np.testing.assert_array_equal(fa[key], fb[key])
+
+
+def test_fp64_tiled_static_matches_oracle():
+    import coolbubble_b200 as cb
+    from oracle import bridge as B
+    d, n, L, c = 3, 128, 32.0, 2.0
+    dt = 0.1 * L / n
+    phi0, pi0 = smooth_noise(d, n, 0.3, seed=13), smooth_noise(d, n, 0.05, seed=14)
+    s = cb.Bubble(cb.make_params(d, n, L, c, dt), phi0, pi0)
+    o = B.Oracle(d, n, L, c, dt, phi0, pi0)
+    for _ in range(3):
+        got = s.step(20, sums=True, local=True)
+        o.step(20)
+        check_sums(got, o.scalars(), n ** d)
+    f, fo = s.fields(), o.fields()
+    for k in ("phi", "pi", "ekin", "egrad", "epot"):
+        assert field_err(f[k], fo[k]) <= FIELD_TOL, k
+
+
+def test_device_error_word_stays_clear():
+    """The bounded waits of the tiled kernel never fired during a normal run."""
+    import coolbubble_b200 as cb
+    d, n, L, c = 3, 256, 32.0, 2.0
+    s = cb.Bubble(cb.make_params(d, n, L, c, 0.1 * L / n, precision="fp32c"), smooth_noise(d, n, 0.1, seed=1))
+    s.step(50, sums=True)
+    assert s.device_error() == 0
