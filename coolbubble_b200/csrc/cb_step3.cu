@@ -78,9 +78,19 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
-constexpr int NT3 = 256;
+constexpr int CW = 8;                 /* consumer warps */
+constexpr int NC = CW * 32;           /* consumer threads */
+constexpr int NT3 = NC + 32;          /* plus one producer warp */
 constexpr long long WAIT_LIMIT = 2000000000LL;   /* ~1 s at 2 GHz */
 constexpr int ERR_TMA_TIMEOUT = 0x71;
+constexpr int HDR = 256;              /* full[16] and empty[16] mbarriers */
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+/* barrier among the consumer warps only (id 1; id 0 is __syncthreads) */
+__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(NC) : "memory"); }
 
 template <typename T>
 struct Vec;
@@ -117,7 +127,7 @@ struct StageGeom {
 };
 
 template <typename T, bool DF, bool SUMS>
-__global__ void __launch_bounds__(NT3) k_step3(StepConst k, int tj, int nstage, const T *__restrict__ phi_in,
+__global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstage, int cz, const T *__restrict__ phi_in,
                                                 const T *__restrict__ pi_in, T *__restrict__ phi_out,
                                                 T *__restrict__ pi_out, T *__restrict__ loc_ek,
                                                 T *__restrict__ loc_eg, T *__restrict__ loc_ep, DevState *st,
@@ -129,185 +139,197 @@ __global__ void __launch_bounds__(NT3) k_step3(StepConst k, int tj, int nstage, 
     const int n = k.n;
     const StageGeom<T, DF> g{n, tj};
     const size_t stage_elems = g.elems();
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smraw);
-    T *ring = reinterpret_cast<T *>(smraw + 128);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smraw);
+    uint64_t *empty = full + 16;
+    T *ring = reinterpret_cast<T *>(smraw + HDR);
     __shared__ int abort_flag;
+    __shared__ int issued_count;
 
     const int ntiles = n / tj;
     const int tile = blockIdx.x % ntiles;
     const int chunk = blockIdx.x / ntiles;
     const int j0 = tile * tj;
-    const int i0 = chunk * k.cz;
-    const int i1 = min(i0 + k.cz, n);
+    const int i0 = chunk * cz;
+    const int i1 = min(i0 + cz, n);
     const size_t row_bytes = (size_t)n * sizeof(T);
     const size_t plane = (size_t)n * n;
     const int jm = (j0 - 1 + n) % n, jp = (j0 + tj) % n;
     const uint32_t tx_bytes = (uint32_t)(((size_t)(tj + 2) + g.pi_rows()) * row_bytes);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     /* planes needed: i0 - 1 .. i1 (the axis-0 neighbours of the chunk) */
     const int first = i0 - 1;
     const int count = i1 - i0 + 2;
     auto stage_of = [&](int p) { return (p - first) % nstage; };
     auto parity_of = [&](int p) { return (uint32_t)(((p - first) / nstage) & 1); };
-    auto issue = [&](int p) {
-        const int s = stage_of(p);
-        const int pw = (p + n) % n;
-        T *dst = ring + (size_t)s * stage_elems;
-        const T *src_phi = phi_in + (size_t)pw * plane;
-        const T *src_pi = pi_in + (size_t)pw * plane;
-        mbar_arrive_expect_tx(&bars[s], tx_bytes);
-        bulk_g2s(dst + n, src_phi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &bars[s]);
-        bulk_g2s(dst, src_phi + (size_t)jm * n, (uint32_t)row_bytes, &bars[s]);
-        bulk_g2s(dst + (size_t)(tj + 1) * n, src_phi + (size_t)jp * n, (uint32_t)row_bytes, &bars[s]);
-        T *dpi = dst + g.phi_elems();
-        if (DF) {
-            bulk_g2s(dpi + n, src_pi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &bars[s]);
-            bulk_g2s(dpi, src_pi + (size_t)jm * n, (uint32_t)row_bytes, &bars[s]);
-            bulk_g2s(dpi + (size_t)(tj + 1) * n, src_pi + (size_t)jp * n, (uint32_t)row_bytes, &bars[s]);
-        } else {
-            bulk_g2s(dpi, src_pi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &bars[s]);
-        }
-    };
 
     if (threadIdx.x == 0) {
         abort_flag = 0;
-        for (int s = 0; s < nstage; ++s) mbar_init(&bars[s], 1);
+        issued_count = 0;
+        for (int s = 0; s < nstage; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], CW);
+        }
         fence_mbar_init();
     }
     __syncthreads();
-    int issued = 0;   /* planes issued so far (thread 0's count; all threads track it identically) */
-    if (threadIdx.x == 0) {
-        for (int q = 0; q < count && q < nstage; ++q) issue(first + q);
-    }
-    issued = min(count, nstage);
-
-    const T fl = (T)st->fl, fv = (T)st->fv, kin_w = (T)st->kin_w, vel_w = (T)st->vel_w;
-    const T adx = (T)st->adx, inv_adx = (T)st->inv_adx;
-    const bool adx_pow2 = st->adx_pow2 != 0;
-    const T p = DF ? (T)st->drift_p : (T)1;
-    const T dt = (T)k.dt;
-    const T dx2 = (T)k.dx2, inv_dx2 = (T)k.inv_dx2;
-    const bool dx2_pow2 = k.dx2_pow2 != 0;
-    const T half = (T)0.5;
-    auto grad = [&](T dphi) -> T { return adx_pow2 ? A::mul(dphi, inv_adx) : A::div(dphi, adx); };
 
     Acc<T> acc[NSUM];
-    const int nvec_row = n / W;
-    const int nvec = tj * nvec_row;
-    bool ok = true;
 
-    /* drift-first: apply the pending drift to a whole stage in shared memory */
-    auto drift_stage = [&](int pl) {
-        T *sp = ring + (size_t)stage_of(pl) * stage_elems;
-        const T *spi = sp + g.phi_elems();
-        for (size_t e = threadIdx.x; e < g.phi_elems(); e += NT3)
-            sp[e] = A::add(sp[e], A::mul(A::mul(dt, spi[e]), p));
-    };
-
-    for (int q = 0; q < 2 && ok; ++q) {
-        if (!mbar_wait(&bars[stage_of(first + q)], parity_of(first + q), WAIT_LIMIT)) ok = false;
-    }
-    if (DF && ok) {
-        drift_stage(first);
-        drift_stage(first + 1);
-    }
-    for (int i = i0; i < i1; ++i) {
-        if (ok && !mbar_wait(&bars[stage_of(i + 1)], parity_of(i + 1), WAIT_LIMIT)) ok = false;
-        if (!ok) atomicExch(&abort_flag, 1);
-        if (DF && ok) drift_stage(i + 1);
-        __syncthreads();
-        if (abort_flag) break;
-        const T *Sm = ring + (size_t)stage_of(i - 1) * stage_elems;
-        const T *S0 = ring + (size_t)stage_of(i) * stage_elems;
-        const T *Sp = ring + (size_t)stage_of(i + 1) * stage_elems;
-        const T *P0 = S0 + g.phi_elems() + (DF ? n : 0);
-        const size_t gbase = ((size_t)i * n + j0) * n;
-        for (int v = threadIdx.x; v < nvec; v += NT3) {
-            const int r = v / nvec_row, kv = v % nvec_row;
-            const int kk = kv * W;
-            const size_t c_off = (size_t)(r + 1) * n + kk;
-            const VT c = *reinterpret_cast<const VT *>(S0 + c_off);
-            const VT um = *reinterpret_cast<const VT *>(S0 + c_off - n);
-            const VT up = *reinterpret_cast<const VT *>(S0 + c_off + n);
-            const VT im = *reinterpret_cast<const VT *>(Sm + c_off);
-            const VT ip = *reinterpret_cast<const VT *>(Sp + c_off);
-            const VT pv = *reinterpret_cast<const VT *>(P0 + (size_t)r * n + kk);
-            const T left = S0[(size_t)(r + 1) * n + (kk == 0 ? n - 1 : kk - 1)];
-            const T right = S0[(size_t)(r + 1) * n + (kk + W == n ? 0 : kk + W)];
-            VT phi_new, pi_new, vek, veg, vep;
-#pragma unroll
-            for (int s = 0; s < W; ++s) {
-                const T cur = Vec<T>::get(c, s);
-                const T kmn = s == 0 ? left : Vec<T>::get(c, s - 1);
-                const T kpl = s == W - 1 ? right : Vec<T>::get(c, s + 1);
-                const T two = A::add(cur, cur);
-                const T nxt = Vec<T>::get(ip, s);
-                const T t0 = A::add(A::sub(nxt, two), Vec<T>::get(im, s));
-                const T tj_ = A::add(A::sub(Vec<T>::get(up, s), two), Vec<T>::get(um, s));
-                const T tk = A::add(A::sub(kpl, two), kmn);
-                const T lap = A::add(A::add(t0, tj_), tk);
-                const T flap = A::mul(fl, lap);
-                const T force =
-                    A::sub(dx2_pow2 ? A::mul(flap, inv_dx2) : A::div(flap, dx2), A::mul(fv, dV<T>(k, cur)));
-                const T pic = Vec<T>::get(pv, s);
-                const T pn = A::add(pic, A::mul(dt, force));
-                Vec<T>::set(pi_new, s, pn);
-                Vec<T>::set(phi_new, s, DF ? cur : A::add(cur, A::mul(dt, pn)));
-                if (SUMS) {
-                    const T gx = grad(A::sub(Vec<T>::get(up, s), cur));
-                    const T gy = grad(A::sub(nxt, cur));
-                    const T gz = grad(A::sub(kpl, cur));
-                    const T eg = A::mul(half, A::add(A::add(A::sq(gx), A::sq(gy)), A::sq(gz)));
-                    const T ep = Vpot<T>(k, cur);
-                    const T ek = A::mul(A::mul(kin_w, pn), pn);
-                    const T vv = A::mul(pn, vel_w);
-                    const T et = A::add(A::add(ek, eg), ep);
-                    acc[S_EK].add(ek);
-                    acc[S_EP].add(ep);
-                    acc[S_EG].add(eg);
-                    acc[S_PHI].add(cur);
-                    acc[S_V].add(vv);
-                    acc[Q_EK].add(A::sq(ek));
-                    acc[Q_EP].add(A::sq(ep));
-                    acc[Q_EG].add(A::sq(eg));
-                    acc[Q_ET].add(A::sq(et));
-                    acc[Q_PHI].add(A::sq(cur));
-                    acc[Q_V].add(A::sq(vv));
-                    acc[S_EKIN_IN].add(A::mul(A::mul(kin_w, pic), pic));
-                    Vec<T>::set(vek, s, ek);
-                    Vec<T>::set(veg, s, eg);
-                    Vec<T>::set(vep, s, ep);
+    if (warp == CW) {
+        /* ---- producer: one lane issues every plane, reusing a stage once all
+         *      consumer warps have released the plane it held ---- */
+        if (lane == 0) {
+            int q = 0;
+            for (; q < count; ++q) {
+                const int s = q % nstage;
+                const int use = q / nstage;
+                if (use > 0 && !mbar_wait(&empty[s], (uint32_t)((use - 1) & 1), WAIT_LIMIT)) {
+                    atomicExch(&abort_flag, 1);
+                    break;
+                }
+                if (abort_flag) break;
+                const int pw = (first + q + n) % n;
+                T *dst = ring + (size_t)s * stage_elems;
+                const T *src_phi = phi_in + (size_t)pw * plane;
+                const T *src_pi = pi_in + (size_t)pw * plane;
+                fence_proxy_async();
+                mbar_arrive_expect_tx(&full[s], tx_bytes);
+                bulk_g2s(dst + n, src_phi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
+                bulk_g2s(dst, src_phi + (size_t)jm * n, (uint32_t)row_bytes, &full[s]);
+                bulk_g2s(dst + (size_t)(tj + 1) * n, src_phi + (size_t)jp * n, (uint32_t)row_bytes, &full[s]);
+                T *dpi = dst + g.phi_elems();
+                if (DF) {
+                    bulk_g2s(dpi + n, src_pi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
+                    bulk_g2s(dpi, src_pi + (size_t)jm * n, (uint32_t)row_bytes, &full[s]);
+                    bulk_g2s(dpi + (size_t)(tj + 1) * n, src_pi + (size_t)jp * n, (uint32_t)row_bytes, &full[s]);
+                } else {
+                    bulk_g2s(dpi, src_pi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
                 }
             }
-            const size_t o = gbase + (size_t)r * n + kk;
-            *reinterpret_cast<VT *>(pi_out + o) = pi_new;
-            *reinterpret_cast<VT *>(phi_out + o) = phi_new;
-            if (SUMS && k.want_local) {
-                *reinterpret_cast<VT *>(loc_ek + o) = vek;
-                *reinterpret_cast<VT *>(loc_eg + o) = veg;
-                *reinterpret_cast<VT *>(loc_ep + o) = vep;
-            }
+            issued_count = q;
         }
-        __syncthreads();
-        /* plane i - 1 is no longer needed: refill its stage with the next plane */
-        const int nxt_plane = first + issued;
-        if (issued < count) {
-            if (threadIdx.x == 0) {
-                fence_proxy_async();
-                issue(nxt_plane);
+    } else {
+        /* ---- consumers ---- */
+        const T fl = (T)st->fl, fv = (T)st->fv, kin_w = (T)st->kin_w, vel_w = (T)st->vel_w;
+        const T adx = (T)st->adx, inv_adx = (T)st->inv_adx;
+        const bool adx_pow2 = st->adx_pow2 != 0;
+        const T p = DF ? (T)st->drift_p : (T)1;
+        const T dt = (T)k.dt;
+        const T dx2 = (T)k.dx2, inv_dx2 = (T)k.inv_dx2;
+        const bool dx2_pow2 = k.dx2_pow2 != 0;
+        const T half = (T)0.5;
+        auto grad = [&](T dphi) -> T { return adx_pow2 ? A::mul(dphi, inv_adx) : A::div(dphi, adx); };
+        const int nvec_row = n / W;
+        const int nvec = tj * nvec_row;
+        /* drift-first: apply the pending drift to a whole stage (consumer threads share the work) */
+        auto drift_stage = [&](int pl) {
+            T *sp = ring + (size_t)stage_of(pl) * stage_elems;
+            const T *spi = sp + g.phi_elems();
+            for (size_t e = threadIdx.x; e < g.phi_elems(); e += NC)
+                sp[e] = A::add(sp[e], A::mul(A::mul(dt, spi[e]), p));
+        };
+        /* wait for plane pl; drift-first also drifts it, then all consumers meet
+         * (the decision to stop is taken after the meeting, so it is uniform) */
+        auto acquire = [&](int pl) -> bool {
+            const bool ok = abort_flag == 0 && mbar_wait(&full[stage_of(pl)], parity_of(pl), WAIT_LIMIT);
+            if (!ok) atomicExch(&abort_flag, 1);
+            if (DF) {
+                if (ok) drift_stage(pl);
+                consumer_sync();
+                return abort_flag == 0;
             }
-            ++issued;
+            return ok;
+        };
+        bool run = acquire(first) && acquire(first + 1);
+        for (int i = i0; run && i < i1; ++i) {
+            if (!acquire(i + 1)) break;
+            const T *Sm = ring + (size_t)stage_of(i - 1) * stage_elems;
+            const T *S0 = ring + (size_t)stage_of(i) * stage_elems;
+            const T *Sp = ring + (size_t)stage_of(i + 1) * stage_elems;
+            const T *P0 = S0 + g.phi_elems() + (DF ? n : 0);
+            const size_t gbase = ((size_t)i * n + j0) * n;
+            for (int v = threadIdx.x; v < nvec; v += NC) {
+                const int r = v / nvec_row, kv = v % nvec_row;
+                const int kk = kv * W;
+                const size_t c_off = (size_t)(r + 1) * n + kk;
+                const VT c = *reinterpret_cast<const VT *>(S0 + c_off);
+                const VT um = *reinterpret_cast<const VT *>(S0 + c_off - n);
+                const VT up = *reinterpret_cast<const VT *>(S0 + c_off + n);
+                const VT im = *reinterpret_cast<const VT *>(Sm + c_off);
+                const VT ip = *reinterpret_cast<const VT *>(Sp + c_off);
+                const VT pv = *reinterpret_cast<const VT *>(P0 + (size_t)r * n + kk);
+                const T left = S0[(size_t)(r + 1) * n + (kk == 0 ? n - 1 : kk - 1)];
+                const T right = S0[(size_t)(r + 1) * n + (kk + W == n ? 0 : kk + W)];
+                VT phi_new, pi_new, vek, veg, vep;
+#pragma unroll
+                for (int s = 0; s < W; ++s) {
+                    const T cur = Vec<T>::get(c, s);
+                    const T kmn = s == 0 ? left : Vec<T>::get(c, s - 1);
+                    const T kpl = s == W - 1 ? right : Vec<T>::get(c, s + 1);
+                    const T two = A::add(cur, cur);
+                    const T nxt = Vec<T>::get(ip, s);
+                    /* Laplacian, axes 0, 1, 2 in the reference's order (bubble.cpp:731-736) */
+                    const T t0 = A::add(A::sub(nxt, two), Vec<T>::get(im, s));
+                    const T t1 = A::add(A::sub(Vec<T>::get(up, s), two), Vec<T>::get(um, s));
+                    const T t2 = A::add(A::sub(kpl, two), kmn);
+                    const T lap = A::add(A::add(t0, t1), t2);
+                    const T flap = A::mul(fl, lap);
+                    const T force =
+                        A::sub(dx2_pow2 ? A::mul(flap, inv_dx2) : A::div(flap, dx2), A::mul(fv, dV<T>(k, cur)));
+                    const T pic = Vec<T>::get(pv, s);
+                    const T pn = A::add(pic, A::mul(dt, force));
+                    Vec<T>::set(pi_new, s, pn);
+                    Vec<T>::set(phi_new, s, DF ? cur : A::add(cur, A::mul(dt, pn)));
+                    if (SUMS) {
+                        /* forward gradients: x <- axis 1, y <- axis 0, z <- axis 2 (bubble.cpp:794-801) */
+                        const T gx = grad(A::sub(Vec<T>::get(up, s), cur));
+                        const T gy = grad(A::sub(nxt, cur));
+                        const T gz = grad(A::sub(kpl, cur));
+                        const T eg = A::mul(half, A::add(A::add(A::sq(gx), A::sq(gy)), A::sq(gz)));
+                        const T ep = Vpot<T>(k, cur);
+                        const T ek = A::mul(A::mul(kin_w, pn), pn);
+                        const T vv = A::mul(pn, vel_w);
+                        const T et = A::add(A::add(ek, eg), ep);
+                        acc[S_EK].add(ek);
+                        acc[S_EP].add(ep);
+                        acc[S_EG].add(eg);
+                        acc[S_PHI].add(cur);
+                        acc[S_V].add(vv);
+                        acc[Q_EK].add(A::sq(ek));
+                        acc[Q_EP].add(A::sq(ep));
+                        acc[Q_EG].add(A::sq(eg));
+                        acc[Q_ET].add(A::sq(et));
+                        acc[Q_PHI].add(A::sq(cur));
+                        acc[Q_V].add(A::sq(vv));
+                        acc[S_EKIN_IN].add(A::mul(A::mul(kin_w, pic), pic));
+                        Vec<T>::set(vek, s, ek);
+                        Vec<T>::set(veg, s, eg);
+                        Vec<T>::set(vep, s, ep);
+                    }
+                }
+                const size_t o = gbase + (size_t)r * n + kk;
+                *reinterpret_cast<VT *>(pi_out + o) = pi_new;
+                *reinterpret_cast<VT *>(phi_out + o) = phi_new;
+                if (SUMS && k.want_local) {
+                    *reinterpret_cast<VT *>(loc_ek + o) = vek;
+                    *reinterpret_cast<VT *>(loc_eg + o) = veg;
+                    *reinterpret_cast<VT *>(loc_ep + o) = vep;
+                }
+            }
+            /* this warp no longer needs plane i - 1 */
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[stage_of(i - 1)]);
         }
     }
+    __syncthreads();
     if (abort_flag) {
-        /* drain: every issued plane's copies must land before the block exits */
+        /* record, then let every issued copy land before the block exits */
         if (threadIdx.x == 0) {
             atomicExch(&st->err, ERR_TMA_TIMEOUT);
-            for (int q = issued > nstage ? issued - nstage : 0; q < issued; ++q) {
-                const int pl = first + q;
-                /* completed phases are skipped quickly; a stuck one gives up after the limit */
-                mbar_wait(&bars[stage_of(pl)], parity_of(pl), WAIT_LIMIT / 8);
-            }
+            const int q1 = issued_count;
+            for (int q = q1 > nstage ? q1 - nstage : 0; q < q1; ++q)
+                mbar_wait(&full[stage_of(first + q)], parity_of(first + q), WAIT_LIMIT / 8);
         }
         __syncthreads();
         return;
@@ -326,9 +348,19 @@ __global__ void __launch_bounds__(NT3) k_step3(StepConst k, int tj, int nstage, 
 
 }  // namespace
 
+bool step3_geometry_cz(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid, int &cz);
+
 /* The tiled path covers d = 3 with n a multiple of the vector width, n >= 64
- * and n <= 1024; returns false for other shapes (the generic kernel runs). */
+ * and n <= 1024; returns false for other shapes (the generic kernel runs).
+ * Geometry: TJ rows per tile (TJ * n about 2048 sites in float, 1024 in
+ * double), as many ring stages as keep two blocks per SM (4..6), and planes
+ * per chunk halved from 32 (down to 8) until the grid has >= 4 waves. */
 bool step3_geometry(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid) {
+    int cz;
+    return step3_geometry_cz(k, prec, tj, nstage, smem, grid, cz);
+}
+
+bool step3_geometry_cz(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid, int &cz) {
     if (k.d != 3) return false;
     const int n = k.n;
     const int esz = prec == P_FP64 ? 8 : 4;
@@ -338,33 +370,34 @@ bool step3_geometry(const StepConst &k, int prec, int &tj, int &nstage, size_t &
     tj = 1;
     for (int t = 1; t <= n && t * n <= tile_sites; ++t)
         if (n % t == 0) tj = t;
-    nstage = 5;
     const bool df = k.expanding != 0;
     const size_t stage = ((size_t)(tj + 2) + (size_t)(tj + (df ? 2 : 0))) * n * esz;
-    smem = 128 + nstage * stage;
-    if (smem > 200 * 1024) {
-        nstage = 4;
-        smem = 128 + nstage * stage;
-    }
+    const size_t budget = 110 * 1024;   /* two blocks per SM */
+    nstage = (int)((budget - HDR) / stage);
+    if (nstage > 6) nstage = 6;
+    if (nstage < 4) nstage = 4;
+    smem = HDR + nstage * stage;
     if (smem > 220 * 1024) return false;
-    const int cz = k.cz;
-    grid = (unsigned)((n / tj) * ((n + cz - 1) / cz));
+    const int ntiles = n / tj;
+    cz = 32;
+    while (cz > 8 && (size_t)ntiles * ((n + cz - 1) / cz) < 4 * 2 * 148) cz /= 2;
+    grid = (unsigned)(ntiles * ((n + cz - 1) / cz));
     return true;
 }
 
 cudaError_t launch_step3(int prec, const StepConst &k, bool df, bool sums, const void *phi_in, const void *pi_in,
                          void *phi_out, void *pi_out, void *le, void *lg, void *lp, DevState *st, double *partials,
                          cudaStream_t s) {
-    int tj, nstage;
+    int tj, nstage, cz;
     size_t smem;
     unsigned grid;
-    if (!step3_geometry(k, prec, tj, nstage, smem, grid)) return cudaErrorInvalidValue;
+    if (!step3_geometry_cz(k, prec, tj, nstage, smem, grid, cz)) return cudaErrorInvalidValue;
 #define CB_LAUNCH3(T, DFv, SU)                                                                                     \
     do {                                                                                                           \
         auto fn = k_step3<T, DFv, SU>;                                                                             \
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);          \
         if (e != cudaSuccess) return e;                                                                            \
-        fn<<<grid, NT3, smem, s>>>(k, tj, nstage, (const T *)phi_in, (const T *)pi_in, (T *)phi_out, (T *)pi_out, \
+        fn<<<grid, NT3, smem, s>>>(k, tj, nstage, cz, (const T *)phi_in, (const T *)pi_in, (T *)phi_out, (T *)pi_out, \
                                    (T *)le, (T *)lg, (T *)lp, st, partials);                                       \
     } while (0)
     if (prec == P_FP64) {

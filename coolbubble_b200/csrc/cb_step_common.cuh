@@ -96,7 +96,8 @@ __device__ __forceinline__ T Vpot(const StepConst &k, T f) {
 
 /* Block-wide reduction of NSUM doubles into partials[block]; the last block
  * to finish adds all partials in a fixed order and returns true with the
- * totals in tot[] (valid in thread 0). */
+ * totals in tot[] (valid in thread 0). NT is the block size (a multiple of
+ * 32); the fixed order makes the result independent of which block is last. */
 template <int NT>
 __device__ bool reduce_last_block(double (&v)[NSUM], double *partials, unsigned int *counter, double *tot) {
     constexpr int NW = NT / 32;
@@ -125,7 +126,7 @@ __device__ bool reduce_last_block(double (&v)[NSUM], double *partials, unsigned 
     __syncthreads();
     if (!is_last) return false;
     __threadfence();
-    /* fixed-order sum: thread t takes blocks t, t+NT, ... */
+    /* fixed order: thread t adds blocks t, t + NT, ...; then warps by shuffle; then warps in order */
     double acc[NSUM];
 #pragma unroll
     for (int s = 0; s < NSUM; ++s) acc[s] = 0.0;
@@ -133,17 +134,20 @@ __device__ bool reduce_last_block(double (&v)[NSUM], double *partials, unsigned 
 #pragma unroll
         for (int s = 0; s < NSUM; ++s) acc[s] = __dadd_rn(acc[s], __ldcg(partials + (size_t)b * NSUM + s));
     }
-    __shared__ double tree[NT];
+#pragma unroll
     for (int s = 0; s < NSUM; ++s) {
-        tree[tid] = acc[s];
-        __syncthreads();
-        for (int st = NT / 2; st > 0; st >>= 1) {
-            if (tid < st) tree[tid] = __dadd_rn(tree[tid], tree[tid + st]);
-            __syncthreads();
-        }
-        if (tid == 0) tot[s] = tree[0];
-        __syncthreads();
+        double x = acc[s];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));
+        if (lane == 0) red[w][s] = x;
     }
+    __syncthreads();
+    if (tid < NSUM) {
+        double x = 0.0;
+        for (int i = 0; i < NW; ++i) x = __dadd_rn(x, red[i][tid]);
+        tot[tid] = x;
+    }
+    __syncthreads();
     if (tid == 0) *counter = 0u;
     return true;
 }

@@ -206,7 +206,8 @@ def test_f32_download_is_rounded_fp64_state():
     dict(d=3, n=96, L=24.0, c=3.0, expansion=0, mpl=200.0, prec="fp64"),
 ])
 def test_tiled_kernel_equals_generic_kernel_fp64(case, monkeypatch):
-    """The TMA-tiled d = 3 kernel does the generic kernel's arithmetic op for op."""
+    """The TMA-tiled d = 3 kernel does the generic kernel's per-site arithmetic op
+    for op (bit-identical fields); only the order of the box sums differs."""
     import coolbubble_b200 as cb
     d, n, L, c = case["d"], case["n"], case["L"], case["c"]
     p = cb.make_params(d, n, L, c, 0.1 * L / n, expansion=case["expansion"], mpl=case["mpl"], precision=case["prec"])
@@ -219,7 +220,7 @@ def test_tiled_kernel_equals_generic_kernel_fp64(case, monkeypatch):
     a = tiled.step(25, sums=True, local=True)
     b = generic.step(25, sums=True, local=True)
     for key in a:
-        assert a[key] == b[key], key
+        assert a[key] == pytest.approx(b[key], rel=1e-14, abs=1e-300), key
     fa, fb = tiled.fields(), generic.fields()
     for key in fa:
         np.testing.assert_array_equal(fa[key], fb[key])
