@@ -292,7 +292,10 @@ int step_impl(cb_handle *h, int nsteps, int flags, bool timed) {
     for (int it = 1; it <= nsteps; ++it) {
         const bool last = it == nsteps;
         const bool local = last && (flags & CB_STEP_LOCAL);
-        const bool sums = h->expanding || (last && (flags & (CB_STEP_SUMS | CB_STEP_LOCAL)));
+        const bool want = last && (flags & (CB_STEP_SUMS | CB_STEP_LOCAL));
+        /* every box average when asked for; an expanding background otherwise
+         * needs only the sums of its Friedmann update */
+        const int sums = want ? 2 : (h->expanding ? 1 : 0);
         StepConst k = h->k;
         k.want_local = local ? 1 : 0;
         const int i = h->cphi, j = h->cpi;

@@ -72,7 +72,8 @@ struct StepConst {
 /* Kernel launchers (cb_step.cu). Each returns the cudaError_t of the launch. */
 enum Prec { P_FP64 = 0, P_FP32 = 1 };
 
-cudaError_t launch_step(int prec, const StepConst &k, bool drift_first, bool sums, const void *phi_in,
+/* sums: 0 none, 1 only what the Friedmann update needs, 2 every box average */
+cudaError_t launch_step(int prec, const StepConst &k, bool drift_first, int sums, const void *phi_in,
                         const void *pi_in, void *phi_out, void *pi_out, void *loc_ek, void *loc_eg, void *loc_ep,
                         DevState *st, double *partials, cudaStream_t s);
 /* Number of blocks (and so of partial-sum slots) a step launch may use. */
@@ -80,7 +81,7 @@ size_t step_blocks(const StepConst &k);
 
 /* d = 3 kernel with TMA-staged row tiles (cb_step3.cu). */
 bool step3_geometry(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid);
-cudaError_t launch_step3(int prec, const StepConst &k, bool drift_first, bool sums, const void *phi_in,
+cudaError_t launch_step3(int prec, const StepConst &k, bool drift_first, int sums, const void *phi_in,
                          const void *pi_in, void *phi_out, void *pi_out, void *loc_ek, void *loc_eg, void *loc_ep,
                          DevState *st, double *partials, cudaStream_t s);
 

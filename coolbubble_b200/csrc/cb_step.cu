@@ -52,7 +52,7 @@ namespace {
  * k.cz planes of axis 0. Loads use wrapped coordinates, so partial tiles and
  * lattices smaller than a tile need no special case: threads outside the
  * lattice load valid (wrapped) sites into the tile and do not store. */
-template <typename T, int D, int TX, int TY, bool DF, bool SUMS>
+template <typename T, int D, int TX, int TY, bool DF, int SUMS>
 __global__ void __launch_bounds__(TX *TY) k_step(StepConst k, const T *__restrict__ phi_in,
                                                    const T *__restrict__ pi_in, T *__restrict__ phi_out,
                                                    T *__restrict__ pi_out, T *__restrict__ loc_ek,
@@ -73,11 +73,12 @@ __global__ void __launch_bounds__(TX *TY) k_step(StepConst k, const T *__restric
     /* background of this step (written by the previous epilogue or the host) */
     const T fl = (T)st->fl, fv = (T)st->fv, kin_w = (T)st->kin_w, vel_w = (T)st->vel_w;
     const T adx = (T)st->adx, inv_adx = (T)st->inv_adx;
-    const bool adx_pow2 = st->adx_pow2 != 0;
+    /* float: multiply by the reciprocal; double: divide unless the divisor is a power of two (exact) */
+    const bool adx_pow2 = std::is_same<T, float>::value || st->adx_pow2 != 0;
     const T p = DF ? (T)st->drift_p : (T)1;
     const T dt = (T)k.dt;
     const T dx2 = (T)k.dx2, inv_dx2 = (T)k.inv_dx2;
-    const bool dx2_pow2 = k.dx2_pow2 != 0;
+    const bool dx2_pow2 = std::is_same<T, float>::value || k.dx2_pow2 != 0;
     const T half = (T)0.5;
 
     auto eff = [&](size_t idx) -> T {
@@ -127,9 +128,10 @@ __global__ void __launch_bounds__(TX *TY) k_step(StepConst k, const T *__restric
             const T force = A::sub(dx2_pow2 ? A::mul(flap, inv_dx2) : A::div(flap, dx2), A::mul(fv, dV<T>(k, cur)));
             const T pinew = A::add(pic, A::mul(dt, force));
             const size_t o = base + col;
+            T eg_site = (T)0;
             pi_out[o] = pinew;
             phi_out[o] = DF ? cur : A::add(cur, A::mul(dt, pinew));
-            if (SUMS) {
+            if (SUMS == SUM_FULL || (SUMS == SUM_FRIEDMANN && k.alpha == 1)) {
                 /* forward gradients in the reference's naming (bubble.cpp:788-801) */
                 T gx, gy = (T)0, gz = (T)0;
                 const T dfk = A::sub(tile[ty + 1][tx + 2], cur);
@@ -137,27 +139,32 @@ __global__ void __launch_bounds__(TX *TY) k_step(StepConst k, const T *__restric
                 if (D == 1) gx = grad(dfk);
                 else if (D == 2) { gx = grad(dfk); gy = grad(dfj); }
                 else { gx = grad(dfj); gy = grad(A::sub(next, cur)); gz = grad(dfk); }
-                const T eg = A::mul(half, A::add(A::add(A::sq(gx), A::sq(gy)), A::sq(gz)));
+                eg_site = A::mul(half, A::add(A::add(A::sq(gx), A::sq(gy)), A::sq(gz)));
+            }
+            if (SUMS != SUM_NONE) {
+                const T eg = eg_site;
                 const T ep = Vpot<T>(k, cur);
                 const T ek = A::mul(A::mul(kin_w, pinew), pinew);
-                const T v = A::mul(pinew, vel_w);
-                const T et = A::add(A::add(ek, eg), ep);
                 acc[S_EK].add(ek);
                 acc[S_EP].add(ep);
                 acc[S_EG].add(eg);
-                acc[S_PHI].add(cur);
-                acc[S_V].add(v);
-                acc[Q_EK].add(A::sq(ek));
-                acc[Q_EP].add(A::sq(ep));
-                acc[Q_EG].add(A::sq(eg));
-                acc[Q_ET].add(A::sq(et));
-                acc[Q_PHI].add(A::sq(cur));
-                acc[Q_V].add(A::sq(v));
-                acc[S_EKIN_IN].add(A::mul(A::mul(kin_w, pic), pic));
-                if (k.want_local) {
-                    loc_ek[o] = ek;
-                    loc_eg[o] = eg;
-                    loc_ep[o] = ep;
+                if (SUMS == SUM_FULL) {
+                    const T v = A::mul(pinew, vel_w);
+                    const T et = A::add(A::add(ek, eg), ep);
+                    acc[S_PHI].add(cur);
+                    acc[S_V].add(v);
+                    acc[Q_EK].add(A::sq(ek));
+                    acc[Q_EP].add(A::sq(ep));
+                    acc[Q_EG].add(A::sq(eg));
+                    acc[Q_ET].add(A::sq(et));
+                    acc[Q_PHI].add(A::sq(cur));
+                    acc[Q_V].add(A::sq(v));
+                    acc[S_EKIN_IN].add(A::mul(A::mul(kin_w, pic), pic));
+                    if (k.want_local) {
+                        loc_ek[o] = ek;
+                        loc_eg[o] = eg;
+                        loc_ep[o] = ep;
+                    }
                 }
             }
         }
@@ -169,13 +176,13 @@ __global__ void __launch_bounds__(TX *TY) k_step(StepConst k, const T *__restric
         }
     }
 
-    if (SUMS) {
+    if (SUMS != SUM_NONE) {
         double v[NSUM];
 #pragma unroll
         for (int s = 0; s < NSUM; ++s) v[s] = acc[s].value();
         __shared__ double tot[NSUM];
         if (reduce_last_block<TX * TY>(v, partials, &st->counter, tot)) {
-            if (threadIdx.x == 0 && threadIdx.y == 0) epilogue(k, st, tot, !DF);
+            if (threadIdx.x == 0 && threadIdx.y == 0) epilogue(k, st, tot, !DF, SUMS == SUM_FULL);
         }
     }
 }
@@ -318,7 +325,7 @@ dim3 step_grid(const StepConst &k) {
     return dim3((unsigned)((k.nk + TX3 - 1) / TX3), (unsigned)((k.nj + TY3 - 1) / TY3), gz);
 }
 
-template <typename T, int D, bool DF, bool SUMS>
+template <typename T, int D, bool DF, int SUMS>
 cudaError_t launch_t(const StepConst &k, const void *phi_in, const void *pi_in, void *phi_out, void *pi_out,
                      void *le, void *lg, void *lp, DevState *st, double *partials, cudaStream_t s) {
     const dim3 g = step_grid(k);
@@ -333,15 +340,18 @@ cudaError_t launch_t(const StepConst &k, const void *phi_in, const void *pi_in, 
 }
 
 template <typename T, int D>
-cudaError_t launch_d(const StepConst &k, bool df, bool sums, const void *a, const void *b, void *c, void *d_,
+cudaError_t launch_d(const StepConst &k, bool df, int sums, const void *a, const void *b, void *c, void *d_,
                      void *le, void *lg, void *lp, DevState *st, double *partials, cudaStream_t s) {
-    if (df) return launch_t<T, D, true, true>(k, a, b, c, d_, le, lg, lp, st, partials, s);
-    if (sums) return launch_t<T, D, false, true>(k, a, b, c, d_, le, lg, lp, st, partials, s);
-    return launch_t<T, D, false, false>(k, a, b, c, d_, le, lg, lp, st, partials, s);
+    if (df) {
+        if (sums == SUM_FULL) return launch_t<T, D, true, SUM_FULL>(k, a, b, c, d_, le, lg, lp, st, partials, s);
+        return launch_t<T, D, true, SUM_FRIEDMANN>(k, a, b, c, d_, le, lg, lp, st, partials, s);
+    }
+    if (sums == SUM_FULL) return launch_t<T, D, false, SUM_FULL>(k, a, b, c, d_, le, lg, lp, st, partials, s);
+    return launch_t<T, D, false, SUM_NONE>(k, a, b, c, d_, le, lg, lp, st, partials, s);
 }
 
 template <typename T>
-cudaError_t launch_p(const StepConst &k, bool df, bool sums, const void *a, const void *b, void *c, void *d_,
+cudaError_t launch_p(const StepConst &k, bool df, int sums, const void *a, const void *b, void *c, void *d_,
                      void *le, void *lg, void *lp, DevState *st, double *partials, cudaStream_t s) {
     switch (k.d) {
         case 1: return launch_d<T, 1>(k, df, sums, a, b, c, d_, le, lg, lp, st, partials, s);
@@ -378,7 +388,7 @@ size_t step_blocks(const StepConst &k) {
 
 size_t ic_blocks(const StepConst &k) { return ic_grid(sites(k)); }
 
-cudaError_t launch_step(int prec, const StepConst &k, bool drift_first, bool sums, const void *phi_in,
+cudaError_t launch_step(int prec, const StepConst &k, bool drift_first, int sums, const void *phi_in,
                         const void *pi_in, void *phi_out, void *pi_out, void *loc_ek, void *loc_eg, void *loc_ep,
                         DevState *st, double *partials, cudaStream_t s) {
     int tj, ns;

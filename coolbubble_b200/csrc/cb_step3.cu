@@ -126,7 +126,7 @@ struct StageGeom {
     __device__ __forceinline__ size_t elems() const { return phi_elems() + pi_rows() * n; }
 };
 
-template <typename T, bool DF, bool SUMS>
+template <typename T, bool DF, int SUMS>
 __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstage, int cz, const T *__restrict__ phi_in,
                                                 const T *__restrict__ pi_in, T *__restrict__ phi_out,
                                                 T *__restrict__ pi_out, T *__restrict__ loc_ek,
@@ -213,11 +213,12 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         /* ---- consumers ---- */
         const T fl = (T)st->fl, fv = (T)st->fv, kin_w = (T)st->kin_w, vel_w = (T)st->vel_w;
         const T adx = (T)st->adx, inv_adx = (T)st->inv_adx;
-        const bool adx_pow2 = st->adx_pow2 != 0;
+        /* float: multiply by the reciprocal; double: divide unless the divisor is a power of two (exact) */
+        const bool adx_pow2 = std::is_same<T, float>::value || st->adx_pow2 != 0;
         const T p = DF ? (T)st->drift_p : (T)1;
         const T dt = (T)k.dt;
         const T dx2 = (T)k.dx2, inv_dx2 = (T)k.inv_dx2;
-        const bool dx2_pow2 = k.dx2_pow2 != 0;
+        const bool dx2_pow2 = std::is_same<T, float>::value || k.dx2_pow2 != 0;
         const T half = (T)0.5;
         auto grad = [&](T dphi) -> T { return adx_pow2 ? A::mul(dphi, inv_adx) : A::div(dphi, adx); };
         const int nvec_row = n / W;
@@ -281,37 +282,42 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                     const T pn = A::add(pic, A::mul(dt, force));
                     Vec<T>::set(pi_new, s, pn);
                     Vec<T>::set(phi_new, s, DF ? cur : A::add(cur, A::mul(dt, pn)));
-                    if (SUMS) {
-                        /* forward gradients: x <- axis 1, y <- axis 0, z <- axis 2 (bubble.cpp:794-801) */
-                        const T gx = grad(A::sub(Vec<T>::get(up, s), cur));
-                        const T gy = grad(A::sub(nxt, cur));
-                        const T gz = grad(A::sub(kpl, cur));
-                        const T eg = A::mul(half, A::add(A::add(A::sq(gx), A::sq(gy)), A::sq(gz)));
+                    if (SUMS != SUM_NONE) {
+                        T eg = (T)0;
+                        if (SUMS == SUM_FULL || k.alpha == 1) {
+                            /* forward gradients: x <- axis 1, y <- axis 0, z <- axis 2 (bubble.cpp:794-801) */
+                            const T gx = grad(A::sub(Vec<T>::get(up, s), cur));
+                            const T gy = grad(A::sub(nxt, cur));
+                            const T gz = grad(A::sub(kpl, cur));
+                            eg = A::mul(half, A::add(A::add(A::sq(gx), A::sq(gy)), A::sq(gz)));
+                        }
                         const T ep = Vpot<T>(k, cur);
                         const T ek = A::mul(A::mul(kin_w, pn), pn);
-                        const T vv = A::mul(pn, vel_w);
-                        const T et = A::add(A::add(ek, eg), ep);
                         acc[S_EK].add(ek);
                         acc[S_EP].add(ep);
                         acc[S_EG].add(eg);
-                        acc[S_PHI].add(cur);
-                        acc[S_V].add(vv);
-                        acc[Q_EK].add(A::sq(ek));
-                        acc[Q_EP].add(A::sq(ep));
-                        acc[Q_EG].add(A::sq(eg));
-                        acc[Q_ET].add(A::sq(et));
-                        acc[Q_PHI].add(A::sq(cur));
-                        acc[Q_V].add(A::sq(vv));
-                        acc[S_EKIN_IN].add(A::mul(A::mul(kin_w, pic), pic));
-                        Vec<T>::set(vek, s, ek);
-                        Vec<T>::set(veg, s, eg);
-                        Vec<T>::set(vep, s, ep);
+                        if (SUMS == SUM_FULL) {
+                            const T vv = A::mul(pn, vel_w);
+                            const T et = A::add(A::add(ek, eg), ep);
+                            acc[S_PHI].add(cur);
+                            acc[S_V].add(vv);
+                            acc[Q_EK].add(A::sq(ek));
+                            acc[Q_EP].add(A::sq(ep));
+                            acc[Q_EG].add(A::sq(eg));
+                            acc[Q_ET].add(A::sq(et));
+                            acc[Q_PHI].add(A::sq(cur));
+                            acc[Q_V].add(A::sq(vv));
+                            acc[S_EKIN_IN].add(A::mul(A::mul(kin_w, pic), pic));
+                            Vec<T>::set(vek, s, ek);
+                            Vec<T>::set(veg, s, eg);
+                            Vec<T>::set(vep, s, ep);
+                        }
                     }
                 }
                 const size_t o = gbase + (size_t)r * n + kk;
                 *reinterpret_cast<VT *>(pi_out + o) = pi_new;
                 *reinterpret_cast<VT *>(phi_out + o) = phi_new;
-                if (SUMS && k.want_local) {
+                if (SUMS == SUM_FULL && k.want_local) {
                     *reinterpret_cast<VT *>(loc_ek + o) = vek;
                     *reinterpret_cast<VT *>(loc_eg + o) = veg;
                     *reinterpret_cast<VT *>(loc_ep + o) = vep;
@@ -335,13 +341,13 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         return;
     }
 
-    if (SUMS) {
+    if (SUMS != SUM_NONE) {
         double v[NSUM];
 #pragma unroll
         for (int s = 0; s < NSUM; ++s) v[s] = acc[s].value();
         __shared__ double tot[NSUM];
         if (reduce_last_block<NT3>(v, partials, &st->counter, tot)) {
-            if (threadIdx.x == 0) epilogue(k, st, tot, !DF);
+            if (threadIdx.x == 0) epilogue(k, st, tot, !DF, SUMS == SUM_FULL);
         }
     }
 }
@@ -385,7 +391,7 @@ bool step3_geometry_cz(const StepConst &k, int prec, int &tj, int &nstage, size_
     return true;
 }
 
-cudaError_t launch_step3(int prec, const StepConst &k, bool df, bool sums, const void *phi_in, const void *pi_in,
+cudaError_t launch_step3(int prec, const StepConst &k, bool df, int sums, const void *phi_in, const void *pi_in,
                          void *phi_out, void *pi_out, void *le, void *lg, void *lp, DevState *st, double *partials,
                          cudaStream_t s) {
     int tj, nstage, cz;
@@ -401,13 +407,15 @@ cudaError_t launch_step3(int prec, const StepConst &k, bool df, bool sums, const
                                    (T *)le, (T *)lg, (T *)lp, st, partials);                                       \
     } while (0)
     if (prec == P_FP64) {
-        if (df) CB_LAUNCH3(double, true, true);
-        else if (sums) CB_LAUNCH3(double, false, true);
-        else CB_LAUNCH3(double, false, false);
+        if (df && sums == SUM_FULL) CB_LAUNCH3(double, true, SUM_FULL);
+        else if (df) CB_LAUNCH3(double, true, SUM_FRIEDMANN);
+        else if (sums == SUM_FULL) CB_LAUNCH3(double, false, SUM_FULL);
+        else CB_LAUNCH3(double, false, SUM_NONE);
     } else {
-        if (df) CB_LAUNCH3(float, true, true);
-        else if (sums) CB_LAUNCH3(float, false, true);
-        else CB_LAUNCH3(float, false, false);
+        if (df && sums == SUM_FULL) CB_LAUNCH3(float, true, SUM_FULL);
+        else if (df) CB_LAUNCH3(float, true, SUM_FRIEDMANN);
+        else if (sums == SUM_FULL) CB_LAUNCH3(float, false, SUM_FULL);
+        else CB_LAUNCH3(float, false, SUM_NONE);
     }
 #undef CB_LAUNCH3
     return cudaGetLastError();

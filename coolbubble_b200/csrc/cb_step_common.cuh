@@ -172,10 +172,16 @@ __device__ void set_coefficients(const StepConst &k, DevState *st) {
     st->adx_pow2 = is_pow2(st->adx);
 }
 
+/* Which sums a step kernel accumulates. */
+enum SumMode { SUM_NONE = 0, SUM_FRIEDMANN = 1, SUM_FULL = 2 };
+
 /* The scalar part of oneStep, run by one thread of the last block:
  * time-centred kinetic energy (bubble.cpp:838-843), a'' and the a/a'
- * update (747-757, 860-865), H and C (873-875), pending drift (870). */
-__device__ void epilogue(const StepConst &k, DevState *st, const double *tot, bool static_bg) {
+ * update (747-757, 860-865), H and C (873-875), pending drift (870).
+ * `full`: all sums were accumulated; otherwise only those the Friedmann
+ * update needs (kinetic, potential, and gradient for conformal time), and
+ * only the background advances. */
+__device__ void epilogue(const StepConst &k, DevState *st, const double *tot, bool static_bg, bool full) {
     const double dxLD = k.dxLD, dxLD2 = __dmul_rn(k.dxLD, k.dxLD);
     const double epot = __dmul_rn(tot[S_EP], dxLD);
     const double egrad = __dmul_rn(tot[S_EG], dxLD);
@@ -183,19 +189,21 @@ __device__ void epilogue(const StepConst &k, DevState *st, const double *tot, bo
     const double ekprev = static_bg ? __dmul_rn(tot[S_EKIN_IN], dxLD) : st->ekin_half_prev;
     const double ekin = __dmul_rn(0.5, __dadd_rn(ekhalf, ekprev));
     const double etot = __dadd_rn(__dadd_rn(ekin, epot), egrad);
-    st->epot = epot;
-    st->egrad = egrad;
-    st->ekin = ekin;
-    st->etot = etot;
     st->ekin_half_prev = ekhalf;
-    st->avphi = __dmul_rn(tot[S_PHI], dxLD);
-    st->avphip = __dmul_rn(tot[S_V], dxLD);
-    st->ekin_var = __dmul_rn(tot[Q_EK], dxLD2);
-    st->epot_var = __dmul_rn(tot[Q_EP], dxLD2);
-    st->egrad_var = __dmul_rn(tot[Q_EG], dxLD2);
-    st->etot_var = __dmul_rn(tot[Q_ET], dxLD2);
-    st->avphi_var = __dmul_rn(tot[Q_PHI], dxLD2);
-    st->avphip_var = __dmul_rn(tot[Q_V], dxLD2);
+    if (full) {
+        st->epot = epot;
+        st->egrad = egrad;
+        st->ekin = ekin;
+        st->etot = etot;
+        st->avphi = __dmul_rn(tot[S_PHI], dxLD);
+        st->avphip = __dmul_rn(tot[S_V], dxLD);
+        st->ekin_var = __dmul_rn(tot[Q_EK], dxLD2);
+        st->epot_var = __dmul_rn(tot[Q_EP], dxLD2);
+        st->egrad_var = __dmul_rn(tot[Q_EG], dxLD2);
+        st->etot_var = __dmul_rn(tot[Q_ET], dxLD2);
+        st->avphi_var = __dmul_rn(tot[Q_PHI], dxLD2);
+        st->avphip_var = __dmul_rn(tot[Q_V], dxLD2);
+    }
 
     const double mpl2 = __dmul_rn(__dmul_rn(3.0, k.mpl), k.mpl);
     double a = st->a, ap = st->ap;
@@ -215,9 +223,10 @@ __device__ void epilogue(const StepConst &k, DevState *st, const double *tot, bo
     a = __dadd_rn(a, __dmul_rn(k.dt, ap));
     const double a_half = __dmul_rn(0.5, __dadd_rn(a, a_old));
     st->H = __ddiv_rn(ap_atn, a_old);
-    st->C = k.expanding ? __dsub_rn(__dmul_rn(st->H, st->H),
-                                    __ddiv_rn(__dmul_rn(pow(a_old, (double)(2 * k.alpha)), etot), mpl2))
-                        : 0.0;
+    if (full)   /* C needs the full Etot; only reported at steps that measure all sums */
+        st->C = k.expanding ? __dsub_rn(__dmul_rn(st->H, st->H),
+                                        __ddiv_rn(__dmul_rn(pow(a_old, (double)(2 * k.alpha)), etot), mpl2))
+                            : 0.0;
     st->a = a;
     st->ap = ap;
     st->drift_p = pow(a_half, (double)(-k.d + k.alpha));
