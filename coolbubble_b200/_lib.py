@@ -24,6 +24,11 @@ class cb_params(C.Structure):
                 ("precision", C.c_int), ("memorysave", C.c_int)]
 
 
+class cb_ic_params(C.Structure):
+    _fields_ = [("mode", C.c_int), ("n_bubbles", C.c_int), ("trad", C.c_double), ("deltar", C.c_double),
+                ("test", C.c_int), ("position_seed", C.c_uint), ("thermal_seed", C.c_uint64)]
+
+
 class cb_scalars(C.Structure):
     _fields_ = [("t", C.c_double), ("a", C.c_double), ("ap", C.c_double), ("H", C.c_double),
                 ("ekin_half_prev", C.c_double)]
@@ -74,6 +79,9 @@ _SIGS = {
     "cb_nbins": (C.c_int, [C.c_int, C.c_int]),
     "cb_power_spectrum": (C.c_int, [_h, _dp, _dp, _dp, C.c_int]),
     "cb_dft_r2c": (C.c_int, [C.c_int, C.c_int, _dp, _dp]),
+    "cb_dft_c2r": (C.c_int, [C.c_int, C.c_int, _dp, _dp]),
+    "cb_initial_condition": (C.c_int, [C.POINTER(cb_params), C.POINTER(cb_ic_params), C.c_char_p, _dp, _dp,
+                                       C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "cb_destroy": (C.c_int, [_h]),
     "cb_last_error": (C.c_char_p, [_h]),
     "cb_status_string": (C.c_char_p, [C.c_int]),

@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(FFT_T) k_fft_rows(Plan pl, const T *__restrict
 /* A leading axis, in place: tiles of C consecutive columns. The array is
  * [outer][n][inner]; the axis has stride `inner`. */
 __global__ void __launch_bounds__(FFT_T) k_fft_cols(Plan pl, double2 *data, size_t outer, size_t inner, int C,
-                                                   const double2 *__restrict__ tw) {
+                                                   const double2 *__restrict__ tw, int inverse) {
     extern __shared__ double2 sm[];
     const int n = pl.n;
     double2 *a = sm, *b = sm + (size_t)n * C;
@@ -191,14 +191,52 @@ __global__ void __launch_bounds__(FFT_T) k_fft_cols(Plan pl, double2 *data, size
     for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
         const int c = idx % C, i = idx / C;
         const size_t q = q0 + c;
-        a[i * C + c] = q < inner ? base[(size_t)i * inner + q] : make_double2(0.0, 0.0);
+        double2 x = q < inner ? base[(size_t)i * inner + q] : make_double2(0.0, 0.0);
+        if (inverse) x.y = -x.y;   /* inverse DFT = conj(DFT(conj(x))) */
+        a[i * C + c] = x;
     }
     __syncthreads();
     const double2 *z = fft_smem(a, b, pl, C, tw);
     for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
         const int c = idx % C, i = idx / C;
         const size_t q = q0 + c;
-        if (q < inner) base[(size_t)i * inner + q] = z[i * C + c];
+        double2 x = z[i * C + c];
+        if (inverse) x.y = -x.y;
+        if (q < inner) base[(size_t)i * inner + q] = x;
+    }
+}
+
+/* Last axis, half-complex to real (unnormalised inverse), C row pairs per
+ * block: rows A, B (n/2+1 stored values each, extended by Hermitian
+ * symmetry, imaginary parts of the self-conjugate entries ignored) form
+ * Z_k = A_k + i B_k, whose inverse DFT is a + i b. */
+__global__ void __launch_bounds__(FFT_T) k_fft_rows_c2r(Plan pl, const double2 *__restrict__ half, size_t rows, int C,
+                                                       const double2 *__restrict__ tw, double *__restrict__ out) {
+    extern __shared__ double2 sm[];
+    const int n = pl.n, h = n / 2 + 1;
+    double2 *a = sm, *b = sm + (size_t)n * C;
+    const size_t p0 = (size_t)blockIdx.x * C;
+    for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
+        const int c = idx / n, k = idx % n;
+        const size_t ra = 2 * (p0 + c), rb = ra + 1;
+        const bool mirror = k >= h;
+        const int kk = mirror ? n - k : k;
+        double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
+        if (ra < rows) A = half[ra * h + kk];
+        if (rb < rows) B = half[rb * h + kk];
+        if (mirror) { A.y = -A.y; B.y = -B.y; }
+        if (kk == 0 || 2 * kk == n) { A.y = 0.0; B.y = 0.0; }
+        /* conj(Z): the forward transform of conj(Z) is conj of the inverse of Z */
+        a[k * C + c] = make_double2(A.x - B.y, -(A.y + B.x));
+    }
+    __syncthreads();
+    const double2 *z = fft_smem(a, b, pl, C, tw);
+    for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
+        const int c = idx / n, i = idx % n;
+        const size_t ra = 2 * (p0 + c), rb = ra + 1;
+        const double2 w = z[i * C + c];
+        if (ra < rows) out[ra * n + i] = w.x;
+        if (rb < rows) out[rb * n + i] = -w.y;
     }
 }
 
@@ -374,10 +412,36 @@ cudaError_t fft_r2c(FftState *f, int prec, const void *field, cudaStream_t s) {
         for (int i = 0; i < ax; ++i) outer *= (size_t)n;
         for (int i = ax + 1; i < d - 1; ++i) inner *= (size_t)n;
         const size_t tiles = outer * ((inner + C - 1) / C);
-        k_fft_cols<<<(unsigned)tiles, FFT_T, sm, s>>>(pl, f->half, outer, inner, C, f->tw);
+        k_fft_cols<<<(unsigned)tiles, FFT_T, sm, s>>>(pl, f->half, outer, inner, C, f->tw, 0);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+/* c2r of f->half (overwritten) into the real array `out` (device, n^d doubles). */
+cudaError_t fft_c2r(FftState *f, double *out, cudaStream_t s) {
+    const int n = f->n, d = f->d;
+    Plan pl = plan_of(*f);
+    size_t rows = 1;
+    for (int i = 0; i < d - 1; ++i) rows *= (size_t)n;
+    const int C = tile_cols(n);
+    const size_t sm = smem_bytes(n, C);
+    const int hh = n / 2 + 1;
+    cudaError_t e = cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    for (int ax = 0; ax < d - 1; ++ax) {
+        size_t outer = 1, inner = (size_t)hh;
+        for (int i = 0; i < ax; ++i) outer *= (size_t)n;
+        for (int i = ax + 1; i < d - 1; ++i) inner *= (size_t)n;
+        const size_t tiles = outer * ((inner + C - 1) / C);
+        k_fft_cols<<<(unsigned)tiles, FFT_T, sm, s>>>(pl, f->half, outer, inner, C, f->tw, 1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    e = cudaFuncSetAttribute(k_fft_rows_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    const size_t pairs = (rows + 1) / 2;
+    k_fft_rows_c2r<<<(unsigned)((pairs + C - 1) / C), FFT_T, sm, s>>>(pl, f->half, rows, C, f->tw, out);
+    return cudaGetLastError();
 }
 
 cudaError_t fft_bins(FftState *f, double L, cudaStream_t s) {
@@ -432,6 +496,32 @@ extern "C" int cb_power_spectrum(cb_handle *h, double *power, double *weight, do
         weight[b] = host[nb + b];
         ksum[b] = host[2 * nb + b];
     }
+    return CB_OK;
+}
+
+/* Standalone c2r (host half-complex in, host real out); used by the thermal
+ * initial condition and for checking the inverse DFT. */
+extern "C" int cb_dft_c2r(int d, int n, const double *in, double *out) {
+    if (d < 1 || d > 3 || n < 2 || !in || !out) return fail(nullptr, CB_EINVAL, "bad arguments to cb_dft_c2r");
+    size_t N = 1;
+    for (int i = 0; i < d; ++i) N *= (size_t)n;
+    cudaStream_t s;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "creating a stream");
+    FftState *f = nullptr;
+    int r = fft_setup(nullptr, f, d, n, s);
+    if (r != CB_OK) { cudaStreamDestroy(s); return r; }
+    double *dev = nullptr;
+    e = cudaMalloc(&dev, N * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(f->half, in, f->half_elems * sizeof(double2), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = fft_c2r(f, dev, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dev, N * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(dev);
+    cudaFree(f->tw); cudaFree(f->half); cudaFree(f->hist); cudaFree(f->bins_out);
+    delete f;
+    cudaStreamDestroy(s);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cb_dft_c2r");
     return CB_OK;
 }
 

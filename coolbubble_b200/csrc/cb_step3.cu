@@ -83,7 +83,7 @@ constexpr int NC = CW * 32;           /* consumer threads */
 constexpr int NT3 = NC + 32;          /* plus one producer warp */
 constexpr long long WAIT_LIMIT = 2000000000LL;   /* ~1 s at 2 GHz */
 constexpr int ERR_TMA_TIMEOUT = 0x71;
-constexpr int HDR = 256;              /* full[16] and empty[16] mbarriers */
+constexpr int HDR = 384;              /* full[16], empty[16] and ready[16] mbarriers */
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -141,6 +141,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
     const size_t stage_elems = g.elems();
     uint64_t *full = reinterpret_cast<uint64_t *>(smraw);
     uint64_t *empty = full + 16;
+    uint64_t *ready = full + 32;   /* drift-first: plane drifted by the producer warp */
     T *ring = reinterpret_cast<T *>(smraw + HDR);
     __shared__ int abort_flag;
     __shared__ int issued_count;
@@ -169,6 +170,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         for (int s = 0; s < nstage; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], CW);
+            mbar_init(&ready[s], 1);
         }
         fence_mbar_init();
     }
@@ -177,37 +179,86 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
     Acc<T> acc[NSUM];
 
     if (warp == CW) {
-        /* ---- producer: one lane issues every plane, reusing a stage once all
-         *      consumer warps have released the plane it held ---- */
-        if (lane == 0) {
-            int q = 0;
-            for (; q < count; ++q) {
+        /* ---- producer warp: lane 0 issues the bulk copies of every plane,
+         *      reusing a stage once all consumer warps released the plane it
+         *      held; for the drift-first ordering the whole warp then applies
+         *      the pending drift to each landed plane and signals `ready` ---- */
+        auto issue = [&](int q) {
+            const int s = q % nstage;
+            const int pw = (first + q + n) % n;
+            T *dst = ring + (size_t)s * stage_elems;
+            const T *src_phi = phi_in + (size_t)pw * plane;
+            const T *src_pi = pi_in + (size_t)pw * plane;
+            fence_proxy_async();
+            mbar_arrive_expect_tx(&full[s], tx_bytes);
+            bulk_g2s(dst + n, src_phi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
+            bulk_g2s(dst, src_phi + (size_t)jm * n, (uint32_t)row_bytes, &full[s]);
+            bulk_g2s(dst + (size_t)(tj + 1) * n, src_phi + (size_t)jp * n, (uint32_t)row_bytes, &full[s]);
+            T *dpi = dst + g.phi_elems();
+            if (DF) {
+                bulk_g2s(dpi + n, src_pi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
+                bulk_g2s(dpi, src_pi + (size_t)jm * n, (uint32_t)row_bytes, &full[s]);
+                bulk_g2s(dpi + (size_t)(tj + 1) * n, src_pi + (size_t)jp * n, (uint32_t)row_bytes, &full[s]);
+            } else {
+                bulk_g2s(dpi, src_pi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
+            }
+        };
+        /* stage reuse: plane q goes where plane q - nstage was, once released */
+        auto free_for = [&](int q) -> bool {
+            const int use = q / nstage;
+            return use == 0 || mbar_wait(&empty[q % nstage], (uint32_t)((use - 1) & 1), WAIT_LIMIT);
+        };
+        if (!DF) {
+            if (lane == 0) {
+                int q = 0;
+                for (; q < count; ++q) {
+                    if (!free_for(q)) { atomicExch(&abort_flag, 1); break; }
+                    if (abort_flag) break;
+                    issue(q);
+                }
+                issued_count = q;
+            }
+        } else {
+            /* drift plane q, then issue plane q + nstage - 2 (whose stage held
+             * plane q - 2: released once the consumers computed plane q - 1,
+             * which needed only planes up to q, already ready) */
+            const int lead = nstage - 2;
+            const T dt = (T)k.dt;
+            const T p = (T)st->drift_p;
+            int q_issued = 0;
+            if (lane == 0) {
+                for (; q_issued < count && q_issued < lead; ++q_issued) issue(q_issued);
+            }
+            bool ok = true;
+            for (int q = 0; q < count; ++q) {
                 const int s = q % nstage;
-                const int use = q / nstage;
-                if (use > 0 && !mbar_wait(&empty[s], (uint32_t)((use - 1) & 1), WAIT_LIMIT)) {
-                    atomicExch(&abort_flag, 1);
+                ok = ok && abort_flag == 0 && mbar_wait(&full[s], parity_of(first + q), WAIT_LIMIT);
+                if (!ok) {
+                    if (lane == 0) atomicExch(&abort_flag, 1);
                     break;
                 }
-                if (abort_flag) break;
-                const int pw = (first + q + n) % n;
-                T *dst = ring + (size_t)s * stage_elems;
-                const T *src_phi = phi_in + (size_t)pw * plane;
-                const T *src_pi = pi_in + (size_t)pw * plane;
-                fence_proxy_async();
-                mbar_arrive_expect_tx(&full[s], tx_bytes);
-                bulk_g2s(dst + n, src_phi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
-                bulk_g2s(dst, src_phi + (size_t)jm * n, (uint32_t)row_bytes, &full[s]);
-                bulk_g2s(dst + (size_t)(tj + 1) * n, src_phi + (size_t)jp * n, (uint32_t)row_bytes, &full[s]);
-                T *dpi = dst + g.phi_elems();
-                if (DF) {
-                    bulk_g2s(dpi + n, src_pi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
-                    bulk_g2s(dpi, src_pi + (size_t)jm * n, (uint32_t)row_bytes, &full[s]);
-                    bulk_g2s(dpi + (size_t)(tj + 1) * n, src_pi + (size_t)jp * n, (uint32_t)row_bytes, &full[s]);
-                } else {
-                    bulk_g2s(dpi, src_pi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
+                T *sp = ring + (size_t)s * stage_elems;
+                const T *spi = sp + g.phi_elems();
+                for (size_t e = lane * W; e < g.phi_elems(); e += 32 * W) {
+                    VT f = *reinterpret_cast<const VT *>(sp + e);
+                    const VT v = *reinterpret_cast<const VT *>(spi + e);
+#pragma unroll
+                    for (int t = 0; t < W; ++t)
+                        Vec<T>::set(f, t, A::add(Vec<T>::get(f, t), A::mul(A::mul(dt, Vec<T>::get(v, t)), p)));
+                    *reinterpret_cast<VT *>(sp + e) = f;
                 }
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&ready[s]);
+                    const int qn = q + lead;
+                    if (qn < count && q_issued == qn) {
+                        if (!free_for(qn)) atomicExch(&abort_flag, 1);
+                        else { issue(qn); ++q_issued; }
+                    }
+                }
+                __syncwarp();
             }
-            issued_count = q;
+            if (lane == 0) issued_count = q_issued;
         }
     } else {
         /* ---- consumers ---- */
@@ -215,7 +266,6 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         const T adx = (T)st->adx, inv_adx = (T)st->inv_adx;
         /* float: multiply by the reciprocal; double: divide unless the divisor is a power of two (exact) */
         const bool adx_pow2 = std::is_same<T, float>::value || st->adx_pow2 != 0;
-        const T p = DF ? (T)st->drift_p : (T)1;
         const T dt = (T)k.dt;
         const T dx2 = (T)k.dx2, inv_dx2 = (T)k.inv_dx2;
         const bool dx2_pow2 = std::is_same<T, float>::value || k.dx2_pow2 != 0;
@@ -223,23 +273,12 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         auto grad = [&](T dphi) -> T { return adx_pow2 ? A::mul(dphi, inv_adx) : A::div(dphi, adx); };
         const int nvec_row = n / W;
         const int nvec = tj * nvec_row;
-        /* drift-first: apply the pending drift to a whole stage (consumer threads share the work) */
-        auto drift_stage = [&](int pl) {
-            T *sp = ring + (size_t)stage_of(pl) * stage_elems;
-            const T *spi = sp + g.phi_elems();
-            for (size_t e = threadIdx.x; e < g.phi_elems(); e += NC)
-                sp[e] = A::add(sp[e], A::mul(A::mul(dt, spi[e]), p));
-        };
-        /* wait for plane pl; drift-first also drifts it, then all consumers meet
-         * (the decision to stop is taken after the meeting, so it is uniform) */
+        /* wait for plane pl: landed (drift-last) or landed and drifted by the
+         * producer warp (drift-first) */
         auto acquire = [&](int pl) -> bool {
-            const bool ok = abort_flag == 0 && mbar_wait(&full[stage_of(pl)], parity_of(pl), WAIT_LIMIT);
+            uint64_t *bar = DF ? &ready[stage_of(pl)] : &full[stage_of(pl)];
+            const bool ok = abort_flag == 0 && mbar_wait(bar, parity_of(pl), WAIT_LIMIT);
             if (!ok) atomicExch(&abort_flag, 1);
-            if (DF) {
-                if (ok) drift_stage(pl);
-                consumer_sync();
-                return abort_flag == 0;
-            }
             return ok;
         };
         bool run = acquire(first) && acquire(first + 1);

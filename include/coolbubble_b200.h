@@ -164,6 +164,36 @@ int cb_power_spectrum(cb_handle *h, double *power, double *weight, double *ksum,
  * interleaved (re, im) doubles. n_grids up to 6144 with prime factors <= 13. */
 int cb_dft_r2c(int d, int n_grids, const double *in, double *out);
 
+/* The inverse of cb_dft_r2c: half-complex in (n^(d-1) * (n/2+1) interleaved
+ * complex values; the imaginary parts of the self-conjugate entries are
+ * ignored, as FFTW's c2r does), unnormalised real out (n^d doubles). */
+int cb_dft_c2r(int d, int n_grids, const double *in, double *out);
+
+/* Initial condition parameters: def.h values the reference fixes at compile
+ * time, plus the two seeds it hard-codes. */
+typedef struct cb_ic_params {
+    int mode;                   /* readxns (def.h:39-44): 1 random bubbles, 0 given positions,
+                                   -1 two diagonal bubbles, -2 one centred bubble, -3 thermal */
+    int n_bubbles;              /* nBubbles (def.h:46), mode 1 */
+    double trad;                /* Trad (def.h:48), mode -3: T = trad * sqrt(2 (c + 6)) */
+    double deltar;              /* DeltaR (def.h:50), mode -1 */
+    int test;                   /* TEST (def.h:51): sine wave around the true vacuum */
+    unsigned int position_seed; /* srand seed of the bubble positions: 42 in the reference (bubble.cpp:401) */
+    uint64_t thermal_seed;      /* base of the thermal streams: 12345 in the reference (bubble.cpp:137) */
+} cb_ic_params;
+
+/* The reference constructor's initial condition on the host (bubble.cpp:184-234,
+ * 324-523): phi0 and pi0 (n^d doubles each, pi0 = 0 except mode -3) at t = 0,
+ * ready for cb_create_from_ic. Bubble placement and periodic images are
+ * bit-identical to the reference's. Mode 1 returns the __xns.dat text it
+ * generated in xns_out (capacity xns_cap, length in *xns_len; both may be
+ * NULL); mode 0 reads its positions from xns_in. Mode -3 runs the inverse
+ * DFT on the current CUDA device. Replaces GenerateNucleationPoints,
+ * NucleateBubblesAtGivenPoints, GenerateThermalFluc and the other IC
+ * routines, and check_PBC / xFunc of gridfuncs.cpp. */
+int cb_initial_condition(const cb_params *p, const cb_ic_params *ic, const char *xns_in, double *phi0, double *pi0,
+                         char *xns_out, size_t xns_cap, size_t *xns_len);
+
 /* Release the handle and its device memory. */
 int cb_destroy(cb_handle *h);
 
