@@ -83,7 +83,7 @@ constexpr int NC = CW * 32;           /* consumer threads */
 constexpr int NT3 = NC + 32;          /* plus one producer warp */
 constexpr long long WAIT_LIMIT = 2000000000LL;   /* ~1 s at 2 GHz */
 constexpr int ERR_TMA_TIMEOUT = 0x71;
-constexpr int HDR = 384;              /* full[16], empty[16] and ready[16] mbarriers */
+constexpr int HDR = 256;              /* full[16] and empty[16] mbarriers */
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -141,7 +141,6 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
     const size_t stage_elems = g.elems();
     uint64_t *full = reinterpret_cast<uint64_t *>(smraw);
     uint64_t *empty = full + 16;
-    uint64_t *ready = full + 32;   /* drift-first: plane drifted by the producer warp */
     T *ring = reinterpret_cast<T *>(smraw + HDR);
     __shared__ int abort_flag;
     __shared__ int issued_count;
@@ -170,7 +169,6 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         for (int s = 0; s < nstage; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], CW);
-            mbar_init(&ready[s], 1);
         }
         fence_mbar_init();
     }
@@ -180,9 +178,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
 
     if (warp == CW) {
         /* ---- producer warp: lane 0 issues the bulk copies of every plane,
-         *      reusing a stage once all consumer warps released the plane it
-         *      held; for the drift-first ordering the whole warp then applies
-         *      the pending drift to each landed plane and signals `ready` ---- */
+         *      reusing a stage once all consumer warps released the plane it held ---- */
         auto issue = [&](int q) {
             const int s = q % nstage;
             const int pw = (first + q + n) % n;
@@ -208,57 +204,14 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
             const int use = q / nstage;
             return use == 0 || mbar_wait(&empty[q % nstage], (uint32_t)((use - 1) & 1), WAIT_LIMIT);
         };
-        if (!DF) {
-            if (lane == 0) {
-                int q = 0;
-                for (; q < count; ++q) {
-                    if (!free_for(q)) { atomicExch(&abort_flag, 1); break; }
-                    if (abort_flag) break;
-                    issue(q);
-                }
-                issued_count = q;
+        if (lane == 0) {
+            int q = 0;
+            for (; q < count; ++q) {
+                if (!free_for(q)) { atomicExch(&abort_flag, 1); break; }
+                if (abort_flag) break;
+                issue(q);
             }
-        } else {
-            /* drift plane q, then issue plane q + nstage - 2 (whose stage held
-             * plane q - 2: released once the consumers computed plane q - 1,
-             * which needed only planes up to q, already ready) */
-            const int lead = nstage - 2;
-            const T dt = (T)k.dt;
-            const T p = (T)st->drift_p;
-            int q_issued = 0;
-            if (lane == 0) {
-                for (; q_issued < count && q_issued < lead; ++q_issued) issue(q_issued);
-            }
-            bool ok = true;
-            for (int q = 0; q < count; ++q) {
-                const int s = q % nstage;
-                ok = ok && abort_flag == 0 && mbar_wait(&full[s], parity_of(first + q), WAIT_LIMIT);
-                if (!ok) {
-                    if (lane == 0) atomicExch(&abort_flag, 1);
-                    break;
-                }
-                T *sp = ring + (size_t)s * stage_elems;
-                const T *spi = sp + g.phi_elems();
-                for (size_t e = lane * W; e < g.phi_elems(); e += 32 * W) {
-                    VT f = *reinterpret_cast<const VT *>(sp + e);
-                    const VT v = *reinterpret_cast<const VT *>(spi + e);
-#pragma unroll
-                    for (int t = 0; t < W; ++t)
-                        Vec<T>::set(f, t, A::add(Vec<T>::get(f, t), A::mul(A::mul(dt, Vec<T>::get(v, t)), p)));
-                    *reinterpret_cast<VT *>(sp + e) = f;
-                }
-                __syncwarp();
-                if (lane == 0) {
-                    mbar_arrive(&ready[s]);
-                    const int qn = q + lead;
-                    if (qn < count && q_issued == qn) {
-                        if (!free_for(qn)) atomicExch(&abort_flag, 1);
-                        else { issue(qn); ++q_issued; }
-                    }
-                }
-                __syncwarp();
-            }
-            if (lane == 0) issued_count = q_issued;
+            issued_count = q;
         }
     } else {
         /* ---- consumers ---- */
@@ -267,16 +220,16 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         /* float: multiply by the reciprocal; double: divide unless the divisor is a power of two (exact) */
         const bool adx_pow2 = std::is_same<T, float>::value || st->adx_pow2 != 0;
         const T dt = (T)k.dt;
+        const T p = DF ? (T)st->drift_p : (T)1;
         const T dx2 = (T)k.dx2, inv_dx2 = (T)k.inv_dx2;
         const bool dx2_pow2 = std::is_same<T, float>::value || k.dx2_pow2 != 0;
         const T half = (T)0.5;
         auto grad = [&](T dphi) -> T { return adx_pow2 ? A::mul(dphi, inv_adx) : A::div(dphi, adx); };
         const int nvec_row = n / W;
         const int nvec = tj * nvec_row;
-        /* wait for plane pl: landed (drift-last) or landed and drifted by the
-         * producer warp (drift-first) */
+        /* wait for plane pl to land */
         auto acquire = [&](int pl) -> bool {
-            uint64_t *bar = DF ? &ready[stage_of(pl)] : &full[stage_of(pl)];
+            uint64_t *bar = &full[stage_of(pl)];
             const bool ok = abort_flag == 0 && mbar_wait(bar, parity_of(pl), WAIT_LIMIT);
             if (!ok) atomicExch(&abort_flag, 1);
             return ok;
@@ -293,14 +246,34 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                 const int r = v / nvec_row, kv = v % nvec_row;
                 const int kk = kv * W;
                 const size_t c_off = (size_t)(r + 1) * n + kk;
-                const VT c = *reinterpret_cast<const VT *>(S0 + c_off);
-                const VT um = *reinterpret_cast<const VT *>(S0 + c_off - n);
-                const VT up = *reinterpret_cast<const VT *>(S0 + c_off + n);
-                const VT im = *reinterpret_cast<const VT *>(Sm + c_off);
-                const VT ip = *reinterpret_cast<const VT *>(Sp + c_off);
+                VT c = *reinterpret_cast<const VT *>(S0 + c_off);
+                VT um = *reinterpret_cast<const VT *>(S0 + c_off - n);
+                VT up = *reinterpret_cast<const VT *>(S0 + c_off + n);
+                VT im = *reinterpret_cast<const VT *>(Sm + c_off);
+                VT ip = *reinterpret_cast<const VT *>(Sp + c_off);
                 const VT pv = *reinterpret_cast<const VT *>(P0 + (size_t)r * n + kk);
-                const T left = S0[(size_t)(r + 1) * n + (kk == 0 ? n - 1 : kk - 1)];
-                const T right = S0[(size_t)(r + 1) * n + (kk + W == n ? 0 : kk + W)];
+                const size_t lo = (size_t)(r + 1) * n + (kk == 0 ? n - 1 : kk - 1);
+                const size_t ro = (size_t)(r + 1) * n + (kk + W == n ? 0 : kk + W);
+                T left = S0[lo];
+                T right = S0[ro];
+                if (DF) {
+                    /* the pending drift phi += (dt pi) p of the previous step (bubble.cpp:867-870),
+                     * applied to every value read; the pi stage rows line up with the phi rows */
+                    const size_t po = g.phi_elems();
+                    auto drift_v = [&](VT &f, const T *base, size_t off) {
+                        const VT v = *reinterpret_cast<const VT *>(base + po + off);
+#pragma unroll
+                        for (int t = 0; t < W; ++t)
+                            Vec<T>::set(f, t, A::add(Vec<T>::get(f, t), A::mul(A::mul(dt, Vec<T>::get(v, t)), p)));
+                    };
+                    drift_v(c, S0, c_off);
+                    drift_v(um, S0, c_off - n);
+                    drift_v(up, S0, c_off + n);
+                    drift_v(im, Sm, c_off);
+                    drift_v(ip, Sp, c_off);
+                    left = A::add(left, A::mul(A::mul(dt, S0[po + lo]), p));
+                    right = A::add(right, A::mul(A::mul(dt, S0[po + ro]), p));
+                }
                 VT phi_new, pi_new, vek, veg, vep;
 #pragma unroll
                 for (int s = 0; s < W; ++s) {
