@@ -83,6 +83,8 @@ _SIGS = {
     "cb_initial_condition": (C.c_int, [C.POINTER(cb_params), C.POINTER(cb_ic_params), C.c_char_p, _dp, _dp,
                                        C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "cb_destroy": (C.c_int, [_h]),
+    "cb_step_static_noalloc": (C.c_int, [C.POINTER(cb_params), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_double, C.POINTER(cb_sums)]),
     "cb_last_error": (C.c_char_p, [_h]),
     "cb_status_string": (C.c_char_p, [C.c_int]),
     "cb_footprint_bytes": (C.c_int64, [C.POINTER(cb_params)]),

@@ -194,6 +194,28 @@ typedef struct cb_ic_params {
 int cb_initial_condition(const cb_params *p, const cb_ic_params *ic, const char *xns_in, double *phi0, double *pi0,
                          char *xns_out, size_t xns_cap, size_t *xns_len);
 
+/* One leapfrog step on device buffers the caller owns, allocating nothing.
+ * No counterpart in the reference (which has no device memory at all): it is
+ * for callers that cannot let a library call cudaMalloc -- applications whose
+ * own pool or arena owns every device byte, request loops that must not take
+ * an allocation's latency or failure in their hot path, or code running under
+ * a fixed memory budget that is already handed out.
+ * phi_in/pi_in hold phi_n and pi_{n-1/2} (n^d elements of the precision in
+ * p: double for CB_FP64, float for CB_FP32C); phi_out/pi_out (distinct
+ * buffers) receive phi_{n+1} and pi_{n+1/2}; *out receives the box averages of
+ * the step, with out->t = t_in + dt. Static background only (expansion off
+ * or d < 3). The step's scratch -- per-block partial sums and the record the
+ * last block finishes the step with -- is a fixed 1 MiB array in the library,
+ * reserved on every device that loads it until the process exits; a lattice
+ * whose step needs more than its 10912 partial-sum rows is rejected with
+ * CB_EINVAL. The first call on a device looks the array's device address up
+ * once (cudaGetSymbolAddress); make that first call before any stream
+ * capture. All calls share the one array and it keeps the last call's
+ * contents, so calls that overlap on the GPU (other host threads, other
+ * streams) race; each call runs on the default stream and waits for its step. */
+int cb_step_static_noalloc(const cb_params *p, const void *phi_in, const void *pi_in, void *phi_out, void *pi_out,
+                           double t_in, cb_sums *out);
+
 /* Release the handle and its device memory. */
 int cb_destroy(cb_handle *h);
 
