@@ -252,9 +252,11 @@ def run_reference_arm(args, w, wname):
 
 
 def timed_steps(s, K):
-    """K steps with the box averages measured every OUT_ENERGY_EVERY steps; device ms."""
+    """K steps with the box averages measured every OUT_ENERGY_EVERY steps;
+    returns (device ms, kernel launches queued)."""
     from coolbubble_b200 import _lib as L
     s.sync()
+    launches0, _ = s.counters()
     L.check(L.lib.cb_timer_start(s._h), s._h)
     done = 0
     while done < K:
@@ -264,7 +266,7 @@ def timed_steps(s, K):
         done += k
     ms = L.C.c_double()
     L.check(L.lib.cb_timer_stop(s._h, L.C.byref(ms)), s._h)
-    return ms.value
+    return ms.value, s.counters()[0] - launches0
 
 
 def e2e_run(w, K, phi_h, pi_h, precision):
@@ -338,7 +340,7 @@ def main():
     time.sleep(0.3)
     barrier(dist)
     clocks.mark()
-    ms = timed_steps(s, args.steps)
+    ms, launches = timed_steps(s, args.steps)
     clocks.mark()
     barrier(dist)
     ms = max_over_ranks(dist, ms)
@@ -361,7 +363,7 @@ def main():
     s64.step(3, sums=True)
     k64 = min(args.steps, 200)
     barrier(dist)
-    ms64 = max_over_ranks(dist, timed_steps(s64, k64))
+    ms64 = max_over_ranks(dist, timed_steps(s64, k64)[0])
     s64.close()
     value64 = N * k64 * ws / (ms64 / 1e3)
 
@@ -371,8 +373,8 @@ def main():
     e2e_val = ws * N * args.steps / max_over_ranks(dist, N * args.steps / e2e_val)
 
     peak, peak_kind = measured_peak()
-    per_launch_ms = ms / args.steps
-    alg_bytes = BYTES_PER_SITE[prec] * N
+    per_launch_ms = ms / launches
+    alg_bytes = BYTES_PER_SITE[prec] * N * args.steps / launches   # per launch: units (site-updates) x 16 B
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
     line = {
         "metric": "lattice site-updates/s", "value": value, "unit": "site-updates/s", "n_gpus": ws,
@@ -381,15 +383,16 @@ def main():
         "config": {"workload": args.workload, "d": d, "n": n, "L": w["L"], "c": w["c"], "dt": dt,
                    "expansion": w["expansion"], "precision": prec, "parallelism": f"replicas{ws}",
                    "l2": "inputs larger than L2 (2 x 512^3 floats = 1 GiB)",
-                   "sums_every": OUT_ENERGY_EVERY, "ic": "seeded gaussian fluctuations, amplitude 0.05"},
+                   "sums_every": OUT_ENERGY_EVERY, "ic": "seeded gaussian fluctuations, amplitude 0.05",
+                   "steps_per_pass": int(os.environ.get("CB_TEMPORAL_BLOCK", "2")) if (prec == "fp32c" and not w["expansion"]) else 1},
         "fp64_value": value64, "fp64_ms_per_step": ms64 / k64, "speedup_vs_fp64": value / value64,
         "hbm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": committed_traffic(args.workload, prec), "peak_source": peak_kind,
-                     "alg_bytes_per_launch": alg_bytes,
+                     "alg_bytes_per_launch": alg_bytes, "launch_ms": per_launch_ms,
                      "fp64_frac": (BYTES_PER_SITE["fp64"] * N / (ms64 / k64 / 1e3) / 1e9) / peak},
         "e2e": {"value": e2e_val, "unit": "site-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": args.steps,
+        "gpu_launches": launches,
         "clocks": clk,
         "final_etot": final["etot"],
     }

@@ -70,6 +70,7 @@ _SIGS = {
     "cb_timer_start": (C.c_int, [_h]),
     "cb_timer_stop": (C.c_int, [_h, _dp]),
     "cb_set_device": (C.c_int, [C.c_int]),
+    "cb_get_counters": (C.c_int, [_h, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "cb_pinned_alloc": (C.c_void_p, [C.c_size_t]),
     "cb_pinned_free": (C.c_int, [C.c_void_p]),
     "cb_get_sums": (C.c_int, [_h, C.POINTER(cb_sums)]),

@@ -92,6 +92,12 @@ class Bubble:
     def sync(self):
         check(L.lib.cb_sync(self._h), self._h)
 
+    def counters(self):
+        """(kernel launches, leapfrog steps) queued by this run so far."""
+        a, b = L.C.c_int64(), L.C.c_int64()
+        check(L.lib.cb_get_counters(self._h, L.C.byref(a), L.C.byref(b)), self._h)
+        return a.value, b.value
+
     def device_error(self):
         code = L.C.c_int()
         check(L.lib.cb_device_error(self._h, L.C.byref(code)), self._h)

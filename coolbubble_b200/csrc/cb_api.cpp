@@ -113,6 +113,10 @@ StepConst make_const(const cb_params *p) {
     k.want_local = 0;
     const char *path = std::getenv("CB_STEP_PATH");
     k.force_generic = (path && std::string(path) == "generic") ? 1 : 0;
+    /* steps per pass of the temporally blocked static kernel; CB_TEMPORAL_BLOCK=1 turns it off */
+    const char *tb = std::getenv("CB_TEMPORAL_BLOCK");
+    k.temporal = tb ? std::atoi(tb) : 2;
+    if (k.temporal < 1 || k.force_generic) k.temporal = 1;
     return k;
 }
 
@@ -289,10 +293,30 @@ int step_impl(cb_handle *h, int nsteps, int flags, bool timed) {
         e = cudaEventRecord(h->ev[0], h->stream);
         if (e != cudaSuccess) return cuda_fail(h, e, "recording an event");
     }
-    for (int it = 1; it <= nsteps; ++it) {
+    /* steps that need nothing reported can run in temporally blocked passes */
+    const bool want_last = (flags & (CB_STEP_SUMS | CB_STEP_LOCAL)) != 0;
+    int tj, ns, cz;
+    size_t sm;
+    unsigned g;
+    const int tl = h->k.temporal;
+    const bool tb_ok = !h->expanding && tl > 1 && step3tb_geometry(h->k, h->prec, tl, tj, ns, sm, g, cz);
+    for (int it = 1; it <= nsteps;) {
+        const int plain_left = nsteps - it + 1 - (want_last ? 1 : 0);
+        if (tb_ok && plain_left >= tl) {
+            const int i = h->cphi, j = h->cpi;
+            e = launch_step3_tb(h->prec, h->k, tl, h->phi[i], h->pi[j], h->phi[1 - i], h->pi[1 - j], h->st, h->stream);
+            if (e != cudaSuccess) return cuda_fail(h, e, "launching the temporally blocked step kernel");
+            h->cphi = 1 - i;
+            h->cpi = 1 - j;
+            for (int q = 0; q < tl; ++q) h->t += h->p.dt;   /* bubble.cpp:871, one addition per step */
+            h->steps_done += tl;
+            h->launches++;
+            it += tl;
+            continue;
+        }
         const bool last = it == nsteps;
         const bool local = last && (flags & CB_STEP_LOCAL);
-        const bool want = last && (flags & (CB_STEP_SUMS | CB_STEP_LOCAL));
+        const bool want = last && want_last;
         /* every box average when asked for; an expanding background otherwise
          * needs only the sums of its Friedmann update */
         const int sums = want ? 2 : (h->expanding ? 1 : 0);
@@ -306,6 +330,8 @@ int step_impl(cb_handle *h, int nsteps, int flags, bool timed) {
         h->cpi = 1 - j;
         h->t += h->p.dt;   /* bubble.cpp:871, accumulated the same way */
         h->steps_done++;
+        h->launches++;
+        ++it;
     }
     if (nsteps > 0) h->pending = h->expanding;
     if (timed) {
@@ -465,6 +491,13 @@ int cb_timer_stop(cb_handle *h, double *device_ms) {
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
     if (e != cudaSuccess) return cuda_fail(h, e, "timing on the run's stream");
     *device_ms = ms;
+    return CB_OK;
+}
+
+int cb_get_counters(cb_handle *h, int64_t *launches, int64_t *steps) {
+    if (!h) return fail(nullptr, CB_EINVAL, "handle is NULL");
+    if (launches) *launches = h->launches;
+    if (steps) *steps = h->steps_done;
     return CB_OK;
 }
 

@@ -33,6 +33,7 @@ struct cb_handle {
     size_t tmp_bytes = 0;
     double t = 0.0;
     long long steps_done = 0;
+    long long launches = 0;   /* kernel launches queued by this run */
     bool pending = false;   /* drift-first: phi is one drift behind the whole step */
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cb::FftState *fft = nullptr;

@@ -67,6 +67,7 @@ struct StepConst {
     int alpha, expanding;
     int want_local;
     int force_generic;  /* 1: always use the generic tile kernel (diagnostics and cross-checks) */
+    int temporal;       /* steps per pass for static float 3-D lattices (1: no temporal blocking) */
 };
 
 /* Kernel launchers (cb_step.cu). Each returns the cudaError_t of the launch. */
@@ -84,6 +85,12 @@ bool step3_geometry(const StepConst &k, int prec, int &tj, int &nstage, size_t &
 cudaError_t launch_step3(int prec, const StepConst &k, bool drift_first, int sums, const void *phi_in,
                          const void *pi_in, void *phi_out, void *pi_out, void *loc_ek, void *loc_eg, void *loc_ep,
                          DevState *st, double *partials, cudaStream_t s);
+
+/* TL steps per pass, static float 3-D lattices (cb_step3_tb.cu). */
+bool step3tb_geometry(const StepConst &k, int prec, int tl, int &tj, int &nstage, size_t &smem, unsigned &grid,
+                      int &cz);
+cudaError_t launch_step3_tb(int prec, const StepConst &k, int tl, const void *phi_in, const void *pi_in,
+                            void *phi_out, void *pi_out, DevState *st, cudaStream_t s);
 
 cudaError_t launch_ic_energies(int prec, const StepConst &k, const void *phi, const void *pi, void *loc_ek,
                                void *loc_eg, void *loc_ep, DevState *st, double *partials, cudaStream_t s);

@@ -27,93 +27,19 @@
 
 #include "cb_internal.h"
 #include "cb_step_common.cuh"
+#include "cb_tma.cuh"
 
 namespace cb {
 
 namespace {
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-/* Bounded wait: false after ~limit cycles. */
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
-    const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > limit) return false;
-    }
-    return true;
-}
-
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-
 constexpr int CW = 8;                 /* consumer warps */
 constexpr int NC = CW * 32;           /* consumer threads */
 constexpr int NT3 = NC + 32;          /* plus one producer warp */
-constexpr long long WAIT_LIMIT = 2000000000LL;   /* ~1 s at 2 GHz */
-constexpr int ERR_TMA_TIMEOUT = 0x71;
 constexpr int HDR = 256;              /* full[16] and empty[16] mbarriers */
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
 
 /* barrier among the consumer warps only (id 1; id 0 is __syncthreads) */
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(NC) : "memory"); }
-
-template <typename T>
-struct Vec;
-template <>
-struct Vec<float> {
-    using V = float4;
-    static constexpr int W = 4;
-    static __device__ __forceinline__ float get(const float4 &v, int s) {
-        return s == 0 ? v.x : s == 1 ? v.y : s == 2 ? v.z : v.w;
-    }
-    static __device__ __forceinline__ void set(float4 &v, int s, float x) {
-        if (s == 0) v.x = x; else if (s == 1) v.y = x; else if (s == 2) v.z = x; else v.w = x;
-    }
-};
-template <>
-struct Vec<double> {
-    using V = double2;
-    static constexpr int W = 2;
-    static __device__ __forceinline__ double get(const double2 &v, int s) { return s == 0 ? v.x : v.y; }
-    static __device__ __forceinline__ void set(double2 &v, int s, double x) {
-        if (s == 0) v.x = x; else v.y = x;
-    }
-};
 
 /* Shared-memory layout of one stage: phi rows [TJ + 2][n] (row 0 and TJ + 1
  * are the halo rows), then pi rows [TJ + 2*DF][n] (drift-first also needs the

@@ -122,6 +122,10 @@ int cb_sync(cb_handle *h);
 int cb_timer_start(cb_handle *h);
 int cb_timer_stop(cb_handle *h, double *device_ms);
 
+/* Kernel launches and leapfrog steps this run has queued so far (temporally
+ * blocked passes advance several steps per launch). */
+int cb_get_counters(cb_handle *h, int64_t *launches, int64_t *steps);
+
 /* Select the CUDA device for the runs this host thread creates next
  * (one process per GPU: call it with the local rank). */
 int cb_set_device(int device);

@@ -250,3 +250,35 @@ def test_device_error_word_stays_clear():
     s = cb.Bubble(cb.make_params(d, n, L, c, 0.1 * L / n, precision="fp32c"), smooth_noise(d, n, 0.1, seed=1))
     s.step(50, sums=True)
     assert s.device_error() == 0
+
+
+@pytest.mark.parametrize("n,L,steps", [(64, 16.0, 41), (96, 24.0, 40), (128, 32.0, 40), (256, 32.0, 80)])
+@pytest.mark.parametrize("tl", [2, 3])
+def test_temporal_blocking_matches_single_step_passes(n, L, steps, tl, monkeypatch):
+    """Static float 3-D runs: TL steps per HBM pass give the same fields as one
+    step per pass (to float rounding) and energies within the FP32C bar."""
+    import coolbubble_b200 as cb
+    from oracle import bridge as B
+    d, c = 3, 2.0
+    dt = 0.1 * L / n
+    phi0, pi0 = smooth_noise(d, n, 0.3, seed=31), smooth_noise(d, n, 0.05, seed=32)
+    p = cb.make_params(d, n, L, c, dt, precision="fp32c", memorysave=1)
+    monkeypatch.setenv("CB_TEMPORAL_BLOCK", str(tl))
+    blocked = cb.Bubble(p, phi0, pi0)
+    monkeypatch.setenv("CB_TEMPORAL_BLOCK", "1")
+    single = cb.Bubble(p, phi0, pi0)
+    monkeypatch.delenv("CB_TEMPORAL_BLOCK")
+    a = blocked.step(steps, sums=True)
+    b = single.step(steps, sums=True)
+    launches, nsteps = blocked.counters()
+    assert nsteps == steps and launches < steps   # passes of tl steps were used
+    assert single.counters() == (steps, steps)
+    fa, fb = blocked.fields(local=False), single.fields(local=False)
+    for k in ("phi", "pi"):
+        assert np.abs(fa[k] - fb[k]).max() <= 1e-5 * np.abs(fb[k]).max(), k
+    o = B.Oracle(d, n, L, c, dt, phi0, pi0)
+    o.step(steps)
+    r = o.scalars()
+    for k, rk in (("etot", "Etot"), ("egrad", "Egradtot"), ("epot", "Epottot")):
+        assert abs(a[k] - r[rk]) <= 1e-5 * abs(r[rk]), k
+    assert a["t"] == b["t"] == r["t"]
