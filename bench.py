@@ -384,7 +384,7 @@ def main():
                    "expansion": w["expansion"], "precision": prec, "parallelism": f"replicas{ws}",
                    "l2": "inputs larger than L2 (2 x 512^3 floats = 1 GiB)",
                    "sums_every": OUT_ENERGY_EVERY, "ic": "seeded gaussian fluctuations, amplitude 0.05",
-                   "steps_per_pass": int(os.environ.get("CB_TEMPORAL_BLOCK", "2")) if (prec == "fp32c" and not w["expansion"]) else 1},
+                   "steps_per_pass": int(os.environ.get("CB_TEMPORAL_BLOCK", "1")) if (prec == "fp32c" and not w["expansion"]) else 1},
         "fp64_value": value64, "fp64_ms_per_step": ms64 / k64, "speedup_vs_fp64": value / value64,
         "hbm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

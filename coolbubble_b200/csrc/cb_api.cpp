@@ -113,9 +113,11 @@ StepConst make_const(const cb_params *p) {
     k.want_local = 0;
     const char *path = std::getenv("CB_STEP_PATH");
     k.force_generic = (path && std::string(path) == "generic") ? 1 : 0;
-    /* steps per pass of the temporally blocked static kernel; CB_TEMPORAL_BLOCK=1 turns it off */
+    /* steps per pass of the temporally blocked static kernel (CB_TEMPORAL_BLOCK=2 or 3 turns
+     * it on; off by default: on B200 it does not yet beat the single-step pass, which runs at
+     * 0.95 of the copy bandwidth) */
     const char *tb = std::getenv("CB_TEMPORAL_BLOCK");
-    k.temporal = tb ? std::atoi(tb) : 2;
+    k.temporal = tb ? std::atoi(tb) : 1;
     if (k.temporal < 1 || k.force_generic) k.temporal = 1;
     return k;
 }

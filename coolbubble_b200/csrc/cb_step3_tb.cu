@@ -41,7 +41,7 @@ namespace cb {
 
 namespace {
 
-constexpr int TB_CW = 8;
+constexpr int TB_CW = 16;
 constexpr int TB_NC = TB_CW * 32;
 constexpr int TB_NT = TB_NC + 32;
 constexpr int TB_HDR = 256;
@@ -52,9 +52,8 @@ template <typename T, int TL>
 __global__ void __launch_bounds__(TB_NT, 1)
     k_step3_tb(StepConst k, int tj, int nstage, int cz, const T *__restrict__ phi_in, const T *__restrict__ pi_in,
                T *__restrict__ phi_out, T *__restrict__ pi_out, DevState *st) {
-    using A = Ar<T>;
-    using VT = typename Vec<T>::V;
-    constexpr int W = Vec<T>::W;
+    static_assert(std::is_same<T, float>::value, "the blocked pass is the float path");
+    constexpr int W = 4;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ int abort_flag;
     __shared__ int issued_count;
@@ -68,11 +67,12 @@ __global__ void __launch_bounds__(TB_NT, 1)
     uint64_t *empty = full + 16;
     T *ring0 = reinterpret_cast<T *>(smraw + TB_HDR);
     T *levels = ring0 + (size_t)nstage * stage_elems;
-    /* level l (1..TL-1): phi ring [3][R_l][n] then pi ring [2][R_l][n] */
+    /* level l (1..TL-1): phi ring [3][R_l][n], then pi ring [2][R_(l+1)][n] holding
+     * only the rows level l+1 reads (the centre R_l - 2 rows of level l) */
     auto rows_of = [&](int l) { return tj + 2 * (TL - l); };
     auto level_base = [&](int l) {
         size_t off = 0;
-        for (int m = 1; m < l; ++m) off += (size_t)5 * rows_of(m) * n;
+        for (int m = 1; m < l; ++m) off += (size_t)(3 * rows_of(m) + 2 * rows_of(m + 1)) * n;
         return levels + off;
     };
 
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(TB_NT, 1)
         };
         auto pi_rows = [&](int s, int p) -> const T * {
             if (s == 0) return ring0 + (size_t)stage_of(p) * stage_elems + (size_t)R0 * n;
-            return level_base(s) + (size_t)3 * rows_of(s) * n + (size_t)((p - pbase) % 2) * rows_of(s) * n;
+            return level_base(s) + (size_t)3 * rows_of(s) * n + (size_t)((p - pbase) % 2) * rows_of(s + 1) * n;
         };
         /* one level: rows [0, rows_of(l)) of level l at plane p from level l-1 */
         auto level = [&](int l, int p) {
@@ -168,57 +168,61 @@ __global__ void __launch_bounds__(TB_NT, 1)
             const int Rl = rows_of(l);
             const T *Sm = phi_rows(s, p - 1), *S0 = phi_rows(s, p), *Sp = phi_rows(s, p + 1);
             const T *P0 = pi_rows(s, p);
-            const int prow_off = s == 0 ? 0 : 1;
+            /* pi of level l-1 holds exactly the rows level l computes (row r at r) */
+            const int prow_off = 0;
             T *out_phi = nullptr, *out_pi = nullptr;
             if (l < TL) {
                 out_phi = level_base(l) + (size_t)((p - pbase) % 3) * Rl * n;
-                out_pi = level_base(l) + (size_t)3 * Rl * n + (size_t)((p - pbase) % 2) * Rl * n;
+                out_pi = level_base(l) + (size_t)3 * Rl * n + (size_t)((p - pbase) % 2) * (Rl - 2) * n;
             }
             const int nv = Rl * nvr;
+            /* packed-pair constants: force = (fl inv_dx2) lap - fv V'(phi),
+             * V'(f) = f (c2 + f (-c3 + f c4)) */
+            const F2 FLX = f2_splat((float)(fl * inv_dx2)), NFV = f2_splat(-(float)fv), DT = f2_splat((float)dt);
+            const F2 C2 = f2_splat((float)k.c2), NC3 = f2_splat(-(float)k.c3), C4 = f2_splat((float)k.c4);
             for (int v = threadIdx.x; v < nv; v += TB_NC) {
                 const int r = nvr_shift >= 0 ? (v >> nvr_shift) : v / nvr;
                 const int kk = (v - r * nvr) * W;
                 const size_t c_off = (size_t)(r + 1) * n + kk;
-                const VT c = *reinterpret_cast<const VT *>(S0 + c_off);
-                const VT um = *reinterpret_cast<const VT *>(S0 + c_off - n);
-                const VT up = *reinterpret_cast<const VT *>(S0 + c_off + n);
-                const VT im = *reinterpret_cast<const VT *>(Sm + c_off);
-                const VT ip = *reinterpret_cast<const VT *>(Sp + c_off);
-                const VT pv = *reinterpret_cast<const VT *>(P0 + (size_t)(r + prow_off) * n + kk);
-                const T left = S0[(size_t)(r + 1) * n + (kk == 0 ? n - 1 : kk - 1)];
-                const T right = S0[(size_t)(r + 1) * n + (kk + W == n ? 0 : kk + W)];
-                VT phi_new, pi_new;
-#pragma unroll
-                for (int t = 0; t < W; ++t) {
-                    const T cur = Vec<T>::get(c, t);
-                    const T kmn = t == 0 ? left : Vec<T>::get(c, t - 1);
-                    const T kpl = t == W - 1 ? right : Vec<T>::get(c, t + 1);
-                    const T two = A::add(cur, cur);
-                    const T t0 = A::add(A::sub(Vec<T>::get(ip, t), two), Vec<T>::get(im, t));
-                    const T t1 = A::add(A::sub(Vec<T>::get(up, t), two), Vec<T>::get(um, t));
-                    const T t2 = A::add(A::sub(kpl, two), kmn);
-                    const T lap = A::add(A::add(t0, t1), t2);
-                    const T force = A::sub(A::mul(A::mul(fl, lap), inv_dx2), A::mul(fv, dV<T>(k, cur)));
-                    const T pn = A::add(Vec<T>::get(pv, t), A::mul(dt, force));
-                    Vec<T>::set(pi_new, t, pn);
-                    Vec<T>::set(phi_new, t, A::add(cur, A::mul(dt, pn)));
-                }
+                /* each 16-byte vector as two packed pairs (sites kk, kk+1) and (kk+2, kk+3) */
+                const ulonglong2 c = *reinterpret_cast<const ulonglong2 *>(S0 + c_off);
+                const ulonglong2 um = *reinterpret_cast<const ulonglong2 *>(S0 + c_off - n);
+                const ulonglong2 up = *reinterpret_cast<const ulonglong2 *>(S0 + c_off + n);
+                const ulonglong2 im = *reinterpret_cast<const ulonglong2 *>(Sm + c_off);
+                const ulonglong2 ip = *reinterpret_cast<const ulonglong2 *>(Sp + c_off);
+                const ulonglong2 pv = *reinterpret_cast<const ulonglong2 *>(P0 + (size_t)(r + prow_off) * n + kk);
+                const float left = S0[(size_t)(r + 1) * n + (kk == 0 ? n - 1 : kk - 1)];
+                const float right = S0[(size_t)(r + 1) * n + (kk + W == n ? 0 : kk + W)];
+                const F2 c01{c.x}, c23{c.y};
+                const F2 km01 = f2_pack(left, f2_lo(c01)), km23 = f2_pack(f2_hi(c01), f2_lo(c23));
+                const F2 kp01 = f2_pack(f2_hi(c01), f2_lo(c23)), kp23 = f2_pack(f2_hi(c23), right);
+                auto site2 = [&](F2 cc, F2 umm, F2 upp, F2 imm, F2 ipp, F2 kmm, F2 kpp, F2 pp, F2 &phi_n, F2 &pi_n) {
+                    const F2 two = f2_add(cc, cc);
+                    const F2 t0 = f2_add(f2_sub(ipp, two), imm);
+                    const F2 t1 = f2_add(f2_sub(upp, two), umm);
+                    const F2 t2 = f2_add(f2_sub(kpp, two), kmm);
+                    const F2 lap = f2_add(f2_add(t0, t1), t2);
+                    const F2 h = f2_fma(cc, f2_fma(cc, C4, NC3), C2);
+                    const F2 force = f2_fma(NFV, f2_mul(cc, h), f2_mul(lap, FLX));
+                    pi_n = f2_fma(DT, force, pp);
+                    phi_n = f2_fma(DT, pi_n, cc);
+                };
+                F2 phi01, pi01, phi23, pi23;
+                site2(c01, F2{um.x}, F2{up.x}, F2{im.x}, F2{ip.x}, km01, kp01, F2{pv.x}, phi01, pi01);
+                site2(c23, F2{um.y}, F2{up.y}, F2{im.y}, F2{ip.y}, km23, kp23, F2{pv.y}, phi23, pi23);
+                const ulonglong2 phi_new = make_ulonglong2(phi01.v, phi23.v);
+                const ulonglong2 pi_new = make_ulonglong2(pi01.v, pi23.v);
                 if (l < TL) {
-                    *reinterpret_cast<VT *>(out_phi + (size_t)r * n + kk) = phi_new;
-                    *reinterpret_cast<VT *>(out_pi + (size_t)r * n + kk) = pi_new;
+                    *reinterpret_cast<ulonglong2 *>(out_phi + (size_t)r * n + kk) = phi_new;
+                    if (r >= 1 && r < Rl - 1)
+                        *reinterpret_cast<ulonglong2 *>(out_pi + (size_t)(r - 1) * n + kk) = pi_new;
                 } else {
                     const size_t o = ((size_t)p * n + j0 + r) * n + kk;
-                    *reinterpret_cast<VT *>(pi_out + o) = pi_new;
-                    *reinterpret_cast<VT *>(phi_out + o) = phi_new;
+                    *reinterpret_cast<ulonglong2 *>(pi_out + o) = pi_new;
+                    *reinterpret_cast<ulonglong2 *>(phi_out + o) = phi_new;
                 }
             }
         };
-        /* The decision to stop must be the same in every consumer thread, or
-         * some would wait at a consumer barrier the others never reach: thread
-         * 0 copies abort_flag into consumer_stop between the level barriers,
-         * and all threads act on that copy after the iteration's last barrier
-         * (thread 0 writes it again only after the next iteration's first
-         * barrier, by which time every thread has read it). */
         bool ok = acquire(pbase) && acquire(pbase + 1);
         for (int q = pbase + 2; q < pbase + count0; ++q) {
             ok = ok && acquire(q);
@@ -258,18 +262,20 @@ bool step3tb_geometry(const StepConst &k, int prec, int tl, int &tj, int &nstage
     const int n = k.n;
     if (n % 4 != 0 || n < 64 || n > 1024) return false;
     const size_t esz = 4;
+    const size_t budget = 225 * 1024;   /* one block per SM: the input ring gets what the levels leave */
     for (int target = 2048; target >= 256; target /= 2) {
         tj = 1;
         for (int t = 1; t <= n && t * n <= target; ++t)
             if (n % t == 0) tj = t;
-        nstage = 4;
         const size_t stage = (size_t)(2 * tj + 4 * tl - 2) * n * esz;
         size_t lev = 0;
-        for (int l = 1; l < tl; ++l) lev += (size_t)5 * (tj + 2 * (tl - l)) * n * esz;
-        smem = TB_HDR + nstage * stage + lev;
-        if (smem <= 200 * 1024) break;
+        for (int l = 1; l < tl; ++l) lev += (size_t)(3 * (tj + 2 * (tl - l)) + 2 * (tj + 2 * (tl - l - 1))) * n * esz;
+        nstage = (int)((budget - TB_HDR - lev) / stage);
+        if (nstage > 8) nstage = 8;
+        smem = TB_HDR + (size_t)nstage * stage + lev;
+        if (nstage >= 5 && smem <= budget) break;
     }
-    if (smem > 200 * 1024) return false;
+    if (nstage < 5 || smem > budget) return false;
     const int ntiles = n / tj;
     cz = 32;
     while (cz > 8 && (size_t)ntiles * ((n + cz - 1) / cz) < 4 * 148) cz /= 2;

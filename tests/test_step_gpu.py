@@ -271,7 +271,7 @@ def test_temporal_blocking_matches_single_step_passes(n, L, steps, tl, monkeypat
     a = blocked.step(steps, sums=True)
     b = single.step(steps, sums=True)
     launches, nsteps = blocked.counters()
-    assert nsteps == steps and launches < steps   # passes of tl steps were used
+    assert nsteps == steps and launches < steps   # passes of tl steps were used (opt-in path)
     assert single.counters() == (steps, steps)
     fa, fb = blocked.fields(local=False), single.fields(local=False)
     for k in ("phi", "pi"):
