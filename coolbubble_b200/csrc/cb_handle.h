@@ -48,6 +48,7 @@ int flush_pending(cb_handle *h);
 int ensure_tmp(cb_handle *h, size_t bytes);
 void destroy_handle(cb_handle *h);
 void free_fft(cb_handle *h);
+int step_impl(cb_handle *h, int nsteps, int flags, bool timed);
 }  // namespace cb
 
 #endif

@@ -220,6 +220,28 @@ int cb_initial_condition(const cb_params *p, const cb_ic_params *ic, const char 
 int cb_step_static_noalloc(const cb_params *p, const void *phi_in, const void *pi_in, void *phi_out, void *pi_out,
                            double t_in, cb_sums *out);
 
+/* ---- ensembles: many runs stepped together --------------------------- */
+
+/* No counterpart in the reference, which runs one lattice per process
+ * (main.cpp:45-50). Groups existing runs (their handles stay valid and keep
+ * owning their memory). Two-dimensional static runs whose fields fit in the
+ * shared memory of a thread-block cluster (float: n <= 512, double: n <= 256)
+ * are stepped resident in shared memory, one launch per size class, with the
+ * CTA size chosen by timing candidates once per class (cached per process);
+ * the other members step on their own streams, concurrently. */
+typedef struct cb_ensemble cb_ensemble;
+int cb_ensemble_create(int count, cb_handle *const *members, cb_ensemble **out);
+
+/* Advance every member nsteps steps. With sums_every > 0, the line of every
+ * sums_every-th step of member m goes to out[m * (nsteps / sums_every) + j]. */
+int cb_ensemble_step(cb_ensemble *e, int nsteps, int sums_every, cb_sums *out);
+
+/* How member m is stepped: the cluster size of its resident class (1..16)
+ * and the CTA size the autotuner chose, or 0, 0 when it steps on its own. */
+int cb_ensemble_member_plan(cb_ensemble *e, int m, int *cluster, int *threads);
+
+int cb_ensemble_destroy(cb_ensemble *e);
+
 /* Release the handle and its device memory. */
 int cb_destroy(cb_handle *h);
 
