@@ -300,16 +300,91 @@ def e2e_run(w, K, phi_h, pi_h, precision):
     return N * K / el, h2d / K, d2h / K
 
 
+def ensemble_members(count, seed):
+    """The ensemble configuration: d = 2, n in {128, 256, 512} in equal thirds,
+    c ~ U[1, 8], half mode 1 with 3-10 bubbles, half mode -3 with Trad ~ U[0.01, 0.1],
+    dt = 0.1 dx; every member seeded."""
+    rng = np.random.default_rng(seed)
+    ns = ([128] * (count // 3) + [256] * (count // 3) + [512] * (count - 2 * (count // 3)))
+    rng.shuffle(ns)
+    specs = []
+    for i, n in enumerate(ns):
+        c = float(rng.uniform(1.0, 8.0))
+        thermal = bool(rng.integers(0, 2))
+        specs.append(dict(n=int(n), c=c, L=float(n) / 8.0, thermal=thermal,
+                          nb=int(rng.integers(3, 11)), trad=float(rng.uniform(0.01, 0.1)),
+                          pos_seed=int(rng.integers(1, 2 ** 31)), th_seed=int(rng.integers(1, 2 ** 62))))
+    return specs
+
+
+def run_ensemble_bench(args):
+    """256 independent d = 2 lattices stepped together (FP32C), and the
+    same ensemble in plain FP64; value = total site-updates/s of the ensemble."""
+    import coolbubble_b200 as cb
+    from coolbubble_b200 import _lib as L
+    from coolbubble_b200.ensemble import Ensemble
+    from coolbubble_b200.ic import initial_condition
+    ws, rank, local = dist_env()
+    dist = init_dist(ws)
+    L.check(L.lib.cb_set_device(local))
+    specs = ensemble_members(256, seed=2026 + rank)
+    starts = []
+    for sp in specs:
+        p = cb.make_params(2, sp["n"], sp["L"], sp["c"], 0.1 * sp["L"] / sp["n"], precision="fp32c", memorysave=1)
+        phi0, pi0, _ = initial_condition(p, mode=-3 if sp["thermal"] else 1, n_bubbles=sp["nb"], trad=sp["trad"],
+                                         position_seed=sp["pos_seed"], thermal_seed=sp["th_seed"])
+        starts.append((phi0, pi0))
+    sites = sum(sp["n"] ** 2 for sp in specs)
+    out = {}
+    for prec in ("fp32c", "fp64"):
+        runs = [cb.Bubble(cb.make_params(2, sp["n"], sp["L"], sp["c"], 0.1 * sp["L"] / sp["n"], precision=prec,
+                                         memorysave=1), a, b) for sp, (a, b) in zip(specs, starts)]
+        ens = Ensemble(runs)
+        plans = [ens.plan(i) for i in range(len(runs))]
+        ens.step(args.warmup, 0)
+        barrier(dist)
+        t0 = time.perf_counter()
+        lines = ens.step(args.steps, OUT_ENERGY_EVERY)
+        el = max_over_ranks(dist, time.perf_counter() - t0)
+        out[prec] = dict(seconds=el, value=ws * sites * args.steps / el, plans=plans, lines=lines)
+        del ens, runs
+    resident = sum(1 for c, _ in out["fp32c"]["plans"] if c > 0)
+    line = {
+        "metric": "lattice site-updates/s", "value": out["fp32c"]["value"], "unit": "site-updates/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * out["fp32c"]["seconds"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "ensemble-d2-256", "members": len(specs), "sites_per_step": sites,
+                   "n_mix": {"128": sum(1 for s in specs if s["n"] == 128), "256": sum(1 for s in specs if s["n"] == 256),
+                             "512": sum(1 for s in specs if s["n"] == 512)},
+                   "thermal_members": sum(1 for s in specs if s["thermal"]), "sums_every": OUT_ENERGY_EVERY,
+                   "resident_members_fp32c": resident,
+                   "timing": "host wall clock around one cb_ensemble_step call (launch, all steps, records back)"},
+        "fp64_value": out["fp64"]["value"], "speedup_vs_fp64": out["fp32c"]["value"] / out["fp64"]["value"],
+        "hbm_equivalent_gbs": out["fp32c"]["value"] * 16 / 1e9,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="thermal-d3-n512", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="thermal-d3-n512", choices=sorted(WORKLOADS) + ["ensemble-d2-256"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (profiling runs)")
     args = ap.parse_args()
+    if args.workload == "ensemble-d2-256":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the ensemble workload has no reference arm: "
+                              "the reference runs one lattice per process"}))
+            return 0
+        return run_ensemble_bench(args)
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         return run_reference_arm(args, w, args.workload)

@@ -343,6 +343,27 @@ int step_impl(cb_handle *h, int nsteps, int flags, bool timed) {
     return CB_OK;
 }
 
+/* The constructor's set-up (bubble.cpp:236-291) on the fields already in
+ * phi[0], pi[0]: initial energies, H0, a'_{-1/2}, back-kick, EkinHalfPrev. */
+int finish_create_from_device_ic(cb_handle *h, cb_sums *initial) {
+    cudaError_t e = cudaMemsetAsync(h->st, 0, sizeof(DevState), h->stream);
+    StepConst k = h->k;
+    k.want_local = h->p.memorysave == 0 ? 1 : 0;
+    if (e == cudaSuccess)
+        e = launch_ic_energies(h->prec, k, h->phi[0], h->pi[0], h->loc[0], h->loc[1], h->loc[2], h->st, h->partials,
+                               h->stream);
+    if (e == cudaSuccess) e = launch_ic_backkick(h->prec, k, h->phi[0], h->pi[0], h->st, h->partials, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "running the set-up kernels");
+    h->t = 0.0;
+    h->cphi = h->cpi = 0;
+    DevState s;
+    int r = read_state(h, s);
+    if (r != CB_OK) return r;
+    if (initial) fill_sums(h, s, initial);
+    release_tmp(h);
+    return CB_OK;
+}
+
 }  // namespace cb
 
 int ensure_events(cb_handle *h) {
@@ -425,27 +446,12 @@ int cb_create_from_ic(const cb_params *p, const double *phi0, const double *pi0,
         destroy_handle(h);
         return r;
     }
-    cudaError_t e = cudaMemsetAsync(h->st, 0, sizeof(DevState), h->stream);
-    StepConst k = h->k;
-    k.want_local = p->memorysave == 0 ? 1 : 0;
-    if (e == cudaSuccess)
-        e = launch_ic_energies(h->prec, k, h->phi[0], h->pi[0], h->loc[0], h->loc[1], h->loc[2], h->st, h->partials,
-                               h->stream);
-    if (e == cudaSuccess) e = launch_ic_backkick(h->prec, k, h->phi[0], h->pi[0], h->st, h->partials, h->stream);
-    if (e != cudaSuccess) {
-        cuda_fail(nullptr, e, "running the set-up kernels");
-        destroy_handle(h);
-        return CB_EDEVICE;
-    }
-    h->t = 0.0;
-    DevState s;
-    if ((r = read_state(h, s)) != CB_OK) {
+    r = finish_create_from_device_ic(h, initial);
+    if (r != CB_OK) {
         g_create_error = h->err;
         destroy_handle(h);
         return r;
     }
-    if (initial) fill_sums(h, s, initial);
-    release_tmp(h);
     *out = h;
     return CB_OK;
 }

@@ -499,6 +499,22 @@ extern "C" int cb_power_spectrum(cb_handle *h, double *power, double *weight, do
     return CB_OK;
 }
 
+namespace cb {
+/* c2r of a host half-complex array into a device real array (n^d doubles). */
+int device_c2r(int d, int n, const double *half_host, double *out_dev, cudaStream_t s) {
+    FftState *f = nullptr;
+    int r = fft_setup(nullptr, f, d, n, s);
+    if (r != CB_OK) return r;
+    cudaError_t e = cudaMemcpyAsync(f->half, half_host, f->half_elems * sizeof(double2), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = fft_c2r(f, out_dev, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(f->tw); cudaFree(f->half); cudaFree(f->hist); cudaFree(f->bins_out);
+    delete f;
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "inverse DFT");
+    return CB_OK;
+}
+}  // namespace cb
+
 /* Standalone c2r (host half-complex in, host real out); used by the thermal
  * initial condition and for checking the inverse DFT. */
 extern "C" int cb_dft_c2r(int d, int n, const double *in, double *out) {

@@ -111,17 +111,28 @@ std::string random_positions(int d, double L, int nb, unsigned seed, const Fits 
     return out;
 }
 
-/* Modes 0 and 1 (bubble.cpp:420-453): one profile per "x y z" entry, read as
- * fscanf("%lf %lf %lf") does, added in file order and capped at phi_C. */
-int add_bubbles_from_text(const char *text, int d, int n, double L, const Fits &f, double *phi, size_t N) {
+/* "x y z" entries as fscanf("%lf %lf %lf") reads them (bubble.cpp:431), up to the first malformed one. */
+int read_positions(const char *text, std::vector<double> &xyz) {
     const char *p = text;
     int count = 0;
+    xyz.clear();
     for (;;) {
         double xn[3];
         int used = 0;
         if (std::sscanf(p, "%lf %lf %lf%n", &xn[0], &xn[1], &xn[2], &used) != 3) break;
         p += used;
+        xyz.insert(xyz.end(), xn, xn + 3);
         ++count;
+    }
+    return count;
+}
+
+/* Modes 0 and 1 (bubble.cpp:420-453): one profile per entry, added in file order and capped at phi_C. */
+int add_bubbles_from_text(const char *text, int d, int n, double L, const Fits &f, double *phi, size_t N) {
+    std::vector<double> xyz;
+    const int count = read_positions(text, xyz);
+    for (int b = 0; b < count; ++b) {
+        const double xn[3] = {xyz[3 * b], xyz[3 * b + 1], xyz[3 * b + 2]};
 #pragma omp parallel for schedule(static)
         for (long long si = 0; si < (long long)N; ++si) {
             double x[3];
@@ -149,13 +160,14 @@ uint64_t stream_seed(uint64_t base, const char *name) {
     return base + off;
 }
 
-/* bubble.cpp:459-523: Gaussian random field with <|f_k|^2> = P(k) per mode
- * (continuum normalisation), inverted to real space and scaled by 1/sqrt(L^d). */
-int thermal_field(int d, int n, double L, double T, double m, bool velocity, uint64_t base, const char *name,
-                  double *field) {
+/* bubble.cpp:459-511: the Fourier modes of a Gaussian random field with
+ * <|f_k|^2> = P(k) per mode (continuum normalisation), per-row streams,
+ * Hermitian completion of the planes j = 0 and j = n/2. */
+int thermal_modes(int d, int n, double L, double T, double m, bool velocity, uint64_t base, const char *name,
+                  std::vector<double> &half) {
     const int h = n / 2 + 1;
     const size_t rows = d == 3 ? (size_t)n * n : (size_t)n;
-    std::vector<double> half(rows * h * 2);
+    half.assign(rows * h * 2, 0.0);
     const uint64_t seed = stream_seed(base, name);
     auto kphys = [&](long long i) { return 2.0 * M_PI * (double)((i <= n / 2) ? i : i - n) / L; };
 #pragma omp parallel for schedule(static)
@@ -173,7 +185,6 @@ int thermal_field(int d, int n, double L, double T, double m, bool velocity, uin
             mode[1] = sigma * normal(gen);
         }
     }
-    /* Hermitian completion on the planes j = 0 and j = n/2 (bubble.cpp:490-511) */
     for (int j : {0, n / 2}) {
         for (size_t r = 0; r < rows; ++r) {
             const size_t partner = d == 2 ? (size_t)((n - (long long)r) % n)
@@ -188,15 +199,34 @@ int thermal_field(int d, int n, double L, double T, double m, bool velocity, uin
             }
         }
     }
+    return CB_OK;
+}
+
+/* bubble.cpp:513-519: inverse DFT to real space and scaling by 1/sqrt(L^d). */
+int thermal_field(int d, int n, double L, double T, double m, bool velocity, uint64_t base, const char *name,
+                  double *field) {
+    std::vector<double> half;
+    thermal_modes(d, n, L, T, m, velocity, base, name, half);
     int st = cb_dft_c2r(d, n, half.data(), field);
     if (st != CB_OK) return st;
     const double norm = 1.0 / std::sqrt(std::pow(L, d));
-    size_t N = rows * (size_t)n;
+    size_t N = (d == 3 ? (size_t)n * n : (size_t)n) * (size_t)n;
     for (size_t i = 0; i < N; ++i) field[i] = field[i] * norm + 0.0;
     return CB_OK;
 }
 
 }  // namespace
+
+namespace cb {
+std::string ic_positions_text(int d, double L, double c, int nb, unsigned seed) {
+    return random_positions(d, L, nb, seed, fits(c, d));
+}
+int ic_thermal_modes(int d, int n, double L, double T, double m, bool velocity, uint64_t base, const char *name,
+                     std::vector<double> &half) {
+    return thermal_modes(d, n, L, T, m, velocity, base, name, half);
+}
+int parse_positions(const char *text, std::vector<double> &xyz) { return read_positions(text, xyz); }
+}  // namespace cb
 
 extern "C" int cb_initial_condition(const cb_params *p, const cb_ic_params *ic, const char *xns_in, double *phi0,
                                     double *pi0, char *xns_out, size_t xns_cap, size_t *xns_len) {

@@ -242,6 +242,68 @@ int cb_ensemble_member_plan(cb_ensemble *e, int m, int *cluster, int *threads);
 
 int cb_ensemble_destroy(cb_ensemble *e);
 
+/* cb_create_from_ic with the initial condition built on the device: the
+ * bubble positions, images and thermal modes are drawn on the host exactly as
+ * cb_initial_condition draws them, the per-site profiles and the inverse DFT
+ * run on the GPU straight into the run's buffers (values agree with the host
+ * version to a few ulp). For admitting many runs quickly. */
+int cb_create_from_seed(const cb_params *p, const cb_ic_params *ic, const char *xns_in, cb_sums *initial,
+                        char *xns_out, size_t xns_cap, size_t *xns_len, cb_handle **out);
+
+/* ---- serving: a request loop with runs resident on the GPU ----------- */
+
+/* No counterpart in the reference (one run per process). A worker thread
+ * admits submitted runs in arrival order while a slot and their device memory
+ * (cb_footprint_bytes plus the initial condition's transient buffers) fit the
+ * budget, builds their starts on the device (cb_create_from_seed), advances
+ * all admitted runs concurrently, each on its own stream, in chunks that end
+ * at their output steps (where the line is recorded), and frees a run's
+ * memory as soon as it finishes. A run's results do not depend on which other
+ * runs share the GPU. The pool is thread-safe. */
+typedef struct cb_pool cb_pool;
+
+typedef struct cb_request {
+    cb_params params;
+    cb_ic_params ic;
+    int nt;            /* steps to run */
+    int sums_every;    /* record the line every this many steps (0: none) */
+    int want_fields;   /* keep phi and pi (float) of the last step */
+} cb_request;
+
+#define CB_REQ_QUEUED 0
+#define CB_REQ_RUNNING 1
+#define CB_REQ_DONE 2
+#define CB_REQ_FAILED 3
+#define CB_REQ_CANCELLED 4
+
+typedef struct cb_pool_stats {
+    int64_t queued, active, completed, failed, cancelled, admitted;
+    int64_t used_bytes, budget_bytes;
+    double site_updates;   /* lattice site-updates done so far */
+    double busy_s;         /* time the worker spent with runs on the GPU */
+    double wall_s;         /* time since cb_pool_create */
+} cb_pool_stats;
+
+int cb_pool_create(int64_t budget_bytes, int max_active, cb_pool **out);
+/* xns_in: positions text for mode 0 (else NULL). Returns at once with an id. */
+int cb_pool_submit(cb_pool *pool, const cb_request *req, const char *xns_in, int64_t *id);
+int cb_pool_status(cb_pool *pool, int64_t id, int *state, int *steps_done);
+/* Wait up to timeout_ms for the run to finish (CB_ETIMEOUT otherwise). */
+int cb_pool_wait(cb_pool *pool, int64_t id, int timeout_ms);
+/* A finished run: its recorded lines, the fields if kept, submit-to-finish
+ * latency, and the error text of a failed run. CB_OK for a completed run. */
+int cb_pool_result(cb_pool *pool, int64_t id, cb_sums *lines, int max_lines, int *nlines, float *phi, float *pi,
+                   double *latency_s, char *err, size_t err_cap);
+int cb_pool_cancel(cb_pool *pool, int64_t id);
+int cb_pool_get_stats(cb_pool *pool, cb_pool_stats *out);
+/* Test hook: make the next admission fail (CB_INJECT_ADMISSION_FAILURE) or
+ * the worker thread stop with an exception (CB_INJECT_WORKER_EXCEPTION).
+ * Host-side only; no device fault is involved. */
+#define CB_INJECT_ADMISSION_FAILURE 1
+#define CB_INJECT_WORKER_EXCEPTION 2
+int cb_pool_inject_failure(cb_pool *pool, int kind);
+int cb_pool_destroy(cb_pool *pool);
+
 /* Release the handle and its device memory. */
 int cb_destroy(cb_handle *h);
 
