@@ -369,16 +369,102 @@ def run_ensemble_bench(args):
     return 0
 
 
+def serving_requests(rate, duration, seed):
+    """The serving stream: Poisson arrivals at `rate` per second for `duration`
+    seconds; d in {2, 3}; n uniform in {64, 128, 192, 256, 384} (d = 3 at most
+    256); c ~ U[1, 8]; nt ~ U[200, 5000]; mode 1 or -3 (seeded); expansion on
+    for half of the d = 3 runs (Mpl = 10)."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t > duration:
+            break
+        d = int(rng.integers(2, 4))
+        ns = [64, 128, 192, 256, 384] if d == 2 else [64, 128, 192, 256]
+        n = int(ns[int(rng.integers(0, len(ns)))])
+        out.append(dict(at=t, d=d, n=n, c=float(rng.uniform(1.0, 8.0)), nt=int(rng.integers(200, 5001)),
+                        thermal=bool(rng.integers(0, 2)), expansion=int(d == 3 and rng.integers(0, 2)),
+                        nb=int(rng.integers(3, 11)), trad=float(rng.uniform(0.01, 0.1)),
+                        pos_seed=int(rng.integers(1, 2 ** 31)), th_seed=int(rng.integers(1, 2 ** 62))))
+    return out
+
+
+def run_serving_bench(args):
+    import coolbubble_b200 as cb
+    from coolbubble_b200 import _lib as L
+    from coolbubble_b200.serving import Pool, ic_params, DONE
+    ws, rank, local = dist_env()
+    dist = init_dist(ws)
+    L.check(L.lib.cb_set_device(local))
+    reqs = serving_requests(args.rate, args.duration, seed=77 + rank)
+    pool = Pool(150 * 10 ** 9, args.slots)
+    ids = []
+    barrier(dist)
+    t0 = time.perf_counter()
+    for r in reqs:
+        delay = r["at"] - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        L_box = r["n"] / 8.0
+        p = cb.make_params(r["d"], r["n"], L_box, r["c"], 0.1 * L_box / r["n"], precision="fp32c", memorysave=1,
+                           expansion=r["expansion"], mpl=10.0)
+        ic = ic_params(mode=-3 if r["thermal"] else 1, n_bubbles=r["nb"], trad=r["trad"], position_seed=r["pos_seed"],
+                       thermal_seed=r["th_seed"])
+        ids.append(pool.submit(p, ic, r["nt"], sums_every=OUT_ENERGY_EVERY))
+    lat, updates, states = [], 0.0, []
+    for rid, r in zip(ids, reqs):
+        pool.wait(rid, 3600 * 1000)
+        res = pool.result(rid)
+        states.append(res["state"])
+        lat.append(res["latency"])
+        if res["state"] == DONE:
+            updates += float(r["n"] ** r["d"]) * r["nt"]
+    el = time.perf_counter() - t0
+    st = pool.stats()
+    pool.close()
+    el = max_over_ranks(dist, el)
+    lat = np.array(lat)
+    line = {
+        "metric": "lattice site-updates/s", "value": ws * updates / el, "unit": "site-updates/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serving", "rate_per_s": args.rate, "arrival_window_s": args.duration,
+                   "requests": len(reqs), "slots": args.slots, "budget_bytes": 150 * 10 ** 9,
+                   "precision": "fp32c", "sums_every": OUT_ENERGY_EVERY},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "max": float(lat.max()), "mean": float(lat.mean())},
+        "completed": int(sum(1 for s_ in states if s_ == DONE)), "failed": int(st["failed"]),
+        "makespan_s": el, "gpu_busy_s": st["busy_s"],
+        "site_updates": updates,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="thermal-d3-n512", choices=sorted(WORKLOADS) + ["ensemble-d2-256"])
+    ap.add_argument("--workload", default="thermal-d3-n512",
+                    choices=sorted(WORKLOADS) + ["ensemble-d2-256", "serving"])
+    ap.add_argument("--rate", type=float, default=10.0, help="serving: arrivals per second")
+    ap.add_argument("--duration", type=float, default=20.0, help="serving: arrival window in seconds")
+    ap.add_argument("--slots", type=int, default=64, help="serving: runs on the GPU at once")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (profiling runs)")
     args = ap.parse_args()
+    if args.workload == "serving":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the serving workload has no reference arm: "
+                              "the reference runs one lattice per process"}))
+            return 0
+        return run_serving_bench(args)
     if args.workload == "ensemble-d2-256":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the ensemble workload has no reference arm: "
