@@ -1,0 +1,341 @@
+/* cb_driver.cpp -- coolbubble_gpu: a whole run on the GPU library with the
+ * reference program's command line, run folder and output files.
+ *
+ * Written against the behaviour of the reference's src/main.cpp (options
+ * main.cpp:68-139, folder name 243-249, stability check 171-183, snapshot
+ * schedule 201-223, loop 274-288) and the writers of src/bubble.cpp
+ * (parameters.dat 1018-1032, EnergyDensities.dat 958-989, spectrum files
+ * 642-709, FullField.dat 993-1006). The compile-time def.h values become
+ * options (--dt, --nbubbles, ...) with def.h's defaults. Snapshots are
+ * written as a text manifest plus raw float32 payloads per dataset
+ * (<file>, <file>.<name>.f32), the layout of the HDF5 stand-in of this
+ * repository's oracle; the datasets and attributes are OutField's
+ * (bubble.cpp:887-954). Plots and videos are not made.
+ */
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <filesystem>
+#include <fstream>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "coolbubble_b200.h"
+
+namespace fs = std::filesystem;
+
+namespace {
+
+struct Options {
+    int D = 2, nGrids = 512, nt = 1000, mode = 1, snapshots = 20;
+    double L = 32, c = 4.0;
+    std::string out = "./";
+    /* def.h values (def.h:33-76) */
+    double dt = 0.004, trad = 0.2, deltar = 0.0, mpl = 200.0;
+    int nbubbles = 5, test = 0, expansion = 0, alpha = 0, memorysave = 0;
+    int precision = CB_FP64;
+    unsigned position_seed = 42;
+    unsigned long long thermal_seed = 12345;
+};
+
+const int kOutEnergyEvery = 40;    /* def.h:65 */
+const int kFull1DFieldEvery = 100; /* def.h:71 */
+
+void usage(const char *prog) {
+    std::cout << "Usage: " << prog << " [options]\n\n"
+              << "  --D <1|2|3>  --L <value>  --nGrids <n>  --nt <n>  --c <value>  --mode <1|0|-1|-2|-3>\n"
+              << "  --snapshots <n>  --out <dir>  --no-plots  --python-dir <d>   (as the reference)\n"
+              << "  --dt <value> (TIME_STEP, 0.004)  --nbubbles <n> (5)  --trad <T> (0.2)  --deltar <x> (0)\n"
+              << "  --test <0|1>  --expansion <0|1>  --alpha <0|1>  --mpl <value> (200)  --memorysave <0|1>\n"
+              << "  --precision <fp64|fp32c>  --position-seed <n> (42)  --thermal-seed <n> (12345)\n";
+}
+
+/* main.cpp:62-66: a number with `p` decimals, cut from std::to_string */
+std::string precistr(double num, int p) {
+    const std::string s = std::to_string(num);
+    return s.substr(0, s.find(".") + p + 1);
+}
+
+bool parse(int argc, char **argv, Options &o) {
+    for (int i = 1; i < argc; ++i) {
+        const std::string a = argv[i];
+        if (a == "-h" || a == "--help") { usage(argv[0]); std::exit(0); }
+        if (a == "--no-plots") continue;
+        if (i + 1 >= argc) { std::cerr << "Error: option " << a << " needs a value (see --help)\n"; return false; }
+        const std::string v = argv[++i];
+        try {
+            if (a == "--D") o.D = std::stoi(v);
+            else if (a == "--L") o.L = std::stod(v);
+            else if (a == "--nGrids") o.nGrids = std::stoi(v);
+            else if (a == "--nt") o.nt = std::stoi(v);
+            else if (a == "--c") o.c = std::stod(v);
+            else if (a == "--mode") o.mode = std::stoi(v);
+            else if (a == "--snapshots") o.snapshots = std::stoi(v);
+            else if (a == "--out") o.out = v;
+            else if (a == "--python-dir") { /* no plots are made */ }
+            else if (a == "--dt") o.dt = std::stod(v);
+            else if (a == "--nbubbles") o.nbubbles = std::stoi(v);
+            else if (a == "--trad") o.trad = std::stod(v);
+            else if (a == "--deltar") o.deltar = std::stod(v);
+            else if (a == "--test") o.test = std::stoi(v);
+            else if (a == "--expansion") o.expansion = std::stoi(v);
+            else if (a == "--alpha") o.alpha = std::stoi(v);
+            else if (a == "--mpl") o.mpl = std::stod(v);
+            else if (a == "--memorysave") o.memorysave = std::stoi(v);
+            else if (a == "--position-seed") o.position_seed = (unsigned)std::stoul(v);
+            else if (a == "--thermal-seed") o.thermal_seed = std::stoull(v);
+            else if (a == "--precision") {
+                if (v == "fp64") o.precision = CB_FP64;
+                else if (v == "fp32c") o.precision = CB_FP32C;
+                else throw std::invalid_argument(v);
+            } else {
+                std::cerr << "Error: unknown option " << a << " (see --help)\n";
+                return false;
+            }
+        } catch (const std::exception &) {
+            std::cerr << "Error: cannot read the value '" << v << "' of option " << a << "\n";
+            return false;
+        }
+    }
+    if (o.D < 1 || o.D > 3) { std::cerr << "Error: --D must be 1, 2 or 3\n"; return false; }
+    if (o.nGrids < 2 || o.L <= 0 || o.nt < 1) { std::cerr << "Error: --nGrids, --L and --nt must be positive\n"; return false; }
+    if (o.mode < -3 || o.mode > 1) { std::cerr << "Error: --mode must be between -3 and 1\n"; return false; }
+    if (o.snapshots < 1) { std::cerr << "Error: --snapshots must be at least 1\n"; return false; }
+    return true;
+}
+
+/* main.cpp:201-223 with SnapshotSpacing = 0: evenly spaced in time */
+std::vector<int> schedule(const Options &o) {
+    const double T = o.nt * o.dt;
+    std::vector<int> steps;
+    for (int k = 1; k <= o.snapshots; ++k) {
+        const double time = T * k / o.snapshots;
+        const int step = std::min(o.nt, std::max(1, (int)std::lround(time / o.dt)));
+        if (steps.empty() || step > steps.back()) steps.push_back(step);
+    }
+    return steps;
+}
+
+std::string four(int n) {
+    char b[16];
+    std::snprintf(b, sizeof b, "%04d", n);
+    return b;
+}
+
+struct Run {
+    Options o;
+    std::string folder;
+    cb_handle *h = nullptr;
+    cb_sums line{};
+    double DeltaV = 1.0;
+    size_t N = 0;
+    bool fail(int st, const char *what) {
+        std::cerr << "Error: " << what << ": " << cb_last_error(h) << " (" << cb_status_string(st) << ")\n";
+        return false;
+    }
+};
+
+/* bubble.cpp:958-965 */
+void init_energy_file(const Run &r) {
+    FILE *fp = std::fopen((r.folder + "/EnergyDensities.dat").c_str(), "w");
+    if (!fp) throw std::runtime_error("Could not open EnergyDensities.dat for writing");
+    std::fprintf(fp, "# c and DeltaV are: %.2f %.4f \n", r.o.c, r.DeltaV);
+    std::fprintf(fp, "# columns: 1 t, 2 a, 3 Etot, 4 Ekin, 5 Egrad, 6 Epot, 7-10 spread of Etot/Ekin/Egrad/Epot,\n");
+    std::fprintf(fp, "#          11 <phi>, 12 spread of <phi>, 13 <phi'>, 14 spread of <phi'>, 15 H, 16 Hubble constraint C = H^2 - rho/(3 Mpl^2)\n");
+    std::fclose(fp);
+}
+
+/* bubble.cpp:977-989: one line of the box averages */
+void energy_line(const Run &r, const cb_sums &s) {
+    FILE *fp = std::fopen((r.folder + "/EnergyDensities.dat").c_str(), "a");
+    if (!fp) return;
+    std::fprintf(fp, "%.6e %.10e %.12e %.12e %.12e %.12e %.6e %.6e %.6e %.6e %.6e %.6e %.6e %.6e %.8e %.8e\n", s.t, s.a,
+                 s.etot, s.ekin, s.egrad, s.epot, std::sqrt(s.etot_var), std::sqrt(s.ekin_var), std::sqrt(s.egrad_var),
+                 std::sqrt(s.epot_var), s.avphi, std::sqrt(s.avphi_var), s.avphip, std::sqrt(s.avphip_var), s.H, s.C);
+    std::fclose(fp);
+}
+
+/* bubble.cpp:1018-1032 */
+void parameters_file(const Run &r) {
+    const Options &o = r.o;
+    const double dx = o.L / o.nGrids;
+    const double rn = o.D == 3 ? 0.823 * std::pow(o.c, 0.203) * 1.3 : 0.823 * std::pow(o.c, 0.203);
+    const double kUV = std::sqrt(double(o.D)) * M_PI / dx;
+    const double kIR = 2 * M_PI / double(o.L);
+    const double kRStar = std::sqrt(double(o.D)) * 4 * M_PI / (double(o.L - 2 * rn));
+    const double kMeff = std::sqrt(2 * (o.c + 6));
+    FILE *fp = std::fopen((r.folder + "/parameters.dat").c_str(), "w");
+    if (!fp) throw std::runtime_error("Could not open parameters.dat for writing");
+    std::fprintf(fp, "# The data in this folder correspond to the following:\n");
+    std::fprintf(fp, " D = %d , L = %.10g,  nGrids = %d , TIME_STEP = %.10g  \n", o.D, o.L, o.nGrids, o.dt);
+    std::fprintf(fp, " c = %.10g , nt = %d,  readxns = %d , expansion = %d  \n", o.c, o.nt, o.mode, o.expansion);
+    std::fprintf(fp, " nb = %d , FFT = %d,  ALPHAVAL = %d , WallTracking = %d  \n", o.nbubbles, 1, o.alpha, 0);
+    std::fprintf(fp, "Mpl = %.10g, memorysave = %d, TEST = %d  \n", o.mpl, o.memorysave, o.test);
+    std::fprintf(fp, " Full1DFieldEvery = %d , Trad = %.10g , fixedseed = %d \n", kFull1DFieldEvery, o.trad, 1);
+    std::fprintf(fp, " kUV = %.10g , kIR = %.10g , kRStar = %.10g , kMeff = %.10g \n", kUV, kIR, kRStar, kMeff);
+    std::fclose(fp);
+}
+
+/* bubble.cpp:887-954: datasets phi, pi (and Ekin, gradphi, potEnergy) as float,
+ * attributes D, L, nGrids, reduc, c, t, a (manifest + raw payload layout). */
+bool snapshot(Run &r, int n) {
+    const Options &o = r.o;
+    std::cout << "snapshot " << n << " at t = " << r.line.t << std::endl;
+    std::vector<float> phi(r.N), pi(r.N), ek, eg, ep;
+    if (o.memorysave == 0) { ek.resize(r.N); eg.resize(r.N); ep.resize(r.N); }
+    int st = cb_get_fields_f32(r.h, phi.data(), pi.data(), o.memorysave == 0 ? ek.data() : nullptr,
+                               o.memorysave == 0 ? eg.data() : nullptr, o.memorysave == 0 ? ep.data() : nullptr);
+    if (st != CB_OK) return r.fail(st, "downloading a snapshot");
+    int reduc = 1;
+    if (o.D == 2 && o.nGrids > 2048) reduc = o.nGrids / 2048;
+    if (o.D == 3 && o.nGrids > 512) reduc = o.nGrids / 512;
+    const int m = (o.nGrids + reduc - 1) / reduc;
+    const std::string path = r.folder + "/_phi_t=" + four(n) + ".h5";
+    std::vector<std::pair<std::string, std::vector<float> *>> sets = {{"phi", &phi}, {"pi", &pi}};
+    if (o.memorysave != 1) sets.insert(sets.end(), {{"Ekin", &ek}, {"gradphi", &eg}, {"potEnergy", &ep}});
+    FILE *man = std::fopen(path.c_str(), "w");
+    if (!man) { std::cerr << "Error: could not write the snapshot " << path << std::endl; return true; }
+    const int n0 = o.D >= 3 ? o.nGrids : 1, n1 = o.D >= 2 ? o.nGrids : 1;
+    for (auto &ds : sets) {
+        std::fprintf(man, "dataset %s %d", ds.first.c_str(), o.D);
+        for (int a = 0; a < o.D; ++a) std::fprintf(man, " %d", m);
+        std::fprintf(man, "\n");
+        std::vector<float> thin;
+        thin.reserve((size_t)std::pow((double)m, o.D));
+        for (int i0 = 0; i0 < n0; i0 += (o.D >= 3 ? reduc : 1))
+            for (int i1 = 0; i1 < n1; i1 += (o.D >= 2 ? reduc : 1))
+                for (int i2 = 0; i2 < o.nGrids; i2 += reduc)
+                    thin.push_back((*ds.second)[((size_t)i0 * n1 + i1) * o.nGrids + i2]);
+        FILE *f = std::fopen((path + "." + ds.first + ".f32").c_str(), "wb");
+        if (f) {
+            std::fwrite(thin.data(), sizeof(float), thin.size(), f);
+            std::fclose(f);
+        }
+    }
+    const std::pair<const char *, double> attrs[] = {{"D", (double)o.D}, {"L", o.L}, {"nGrids", (double)o.nGrids},
+                                                     {"reduc", (double)reduc}, {"c", o.c}, {"t", r.line.t},
+                                                     {"a", r.line.a}};
+    for (auto &at : attrs) std::fprintf(man, "attr %s %.17g\n", at.first, at.second);
+    std::fclose(man);
+    /* bubble.cpp:642-709: the power spectrum file */
+    const int nb = cb_nbins(o.D, o.nGrids);
+    std::vector<double> pw(nb), ws(nb), ks(nb);
+    st = cb_power_spectrum(r.h, pw.data(), ws.data(), ks.data(), nb);
+    if (st != CB_OK) return r.fail(st, "power spectrum");
+    std::fstream dat((r.folder + "/_phi_k_t=" + four(n) + ".dat").c_str(), std::ios::out);
+    dat << "# t    a        (then one line per |k| bin: k_comoving  k_physical  Delta(k))" << std::endl;
+    dat << r.line.t << " " << r.line.a << std::endl;
+    for (int b = 0; b < nb; ++b)
+        if (ws[b] > 0) {
+            const double kMean = ks[b] / ws[b];
+            dat << kMean << "   " << kMean / r.line.a << "   " << pw[b] / ws[b] << std::endl;
+        }
+    return true;
+}
+
+/* bubble.cpp:993-1006 (1-D): the whole field as one line */
+bool full_field(Run &r) {
+    std::vector<double> phi(r.N);
+    int st = cb_get_fields(r.h, phi.data(), nullptr, nullptr, nullptr, nullptr);
+    if (st != CB_OK) return r.fail(st, "downloading the field");
+    FILE *fp = std::fopen((r.folder + "/FullField.dat").c_str(), "a");
+    if (!fp) return true;
+    for (double v : phi) std::fprintf(fp, "%.5f ", v);
+    std::fprintf(fp, "\n");
+    std::fclose(fp);
+    return true;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    const auto start = std::chrono::high_resolution_clock::now();
+    Run r;
+    Options &o = r.o;
+    if (!parse(argc, argv, o)) return 1;
+    const std::string name = "Sim" + std::to_string(o.D) + "_D_" + "nt_" + std::to_string(o.nt) + "_dt_" +
+                             precistr(o.dt, 5) + "_nGrids_" + std::to_string(o.nGrids) + "_L_" + precistr(o.L, 1) +
+                             "_Mode_" + std::to_string(o.mode) + "_nB_" + std::to_string(o.nbubbles) + "_c_" +
+                             precistr(o.c, 2) + "_FFT_" + std::to_string(1) +
+                             (o.D == 1 ? "_Full1DFieldEvery_" + std::to_string(kFull1DFieldEvery) : "") + "_Mpl_" +
+                             std::to_string(int(o.mpl));
+    r.folder = (fs::path(o.out) / name).string();
+    const double dx = double(o.L) / o.nGrids;
+    const double dtmax = dx / std::sqrt(o.D);
+    if (!(o.dt < dtmax)) {
+        std::cout << "Stability condition dt < dx/sqrt(D) is not satisfied (dt = " << o.dt
+                  << ", dx/sqrt(D) = " << dtmax << "). Stopping." << std::endl;
+        return 1;
+    }
+    std::cout << "Stability condition dt < dx/sqrt(D) is satisfied." << std::endl;
+    fs::create_directories(r.folder);
+    std::cout << "Output folder: " << r.folder << std::endl;
+    r.N = 1;
+    for (int a = 0; a < o.D; ++a) r.N *= (size_t)o.nGrids;
+
+    cb_params p = {o.D, o.nGrids, o.L, o.c, o.dt, o.alpha, o.expansion, o.mpl, r.DeltaV, o.precision, o.memorysave};
+    cb_ic_params ic = {o.mode, o.nbubbles, o.trad, o.deltar, o.test, o.position_seed, o.thermal_seed};
+    std::vector<double> phi0(r.N), pi0(r.N);
+    std::string xns_in;
+    if (o.mode == 0 && o.D > 1 && !o.test) {
+        std::ifstream f(r.folder + "/__xns.dat");
+        if (!f) {
+            std::cerr << "Error: mode 0 needs the bubble positions in " << r.folder << "/__xns.dat (one \"x y z\" per line)."
+                      << std::endl;
+            return 1;
+        }
+        xns_in.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+    }
+    std::vector<char> xns(64 * 8 * (size_t)std::max(1, o.nbubbles) + 64);
+    size_t xlen = 0;
+    int st = cb_initial_condition(&p, &ic, xns_in.empty() ? nullptr : xns_in.c_str(), phi0.data(), pi0.data(),
+                                  xns.data(), xns.size(), &xlen);
+    if (st != CB_OK) { std::cerr << "Error: initial condition: " << cb_last_error(nullptr) << "\n"; return 1; }
+    if (o.mode == 1 && o.D > 1 && !o.test) {
+        FILE *f = std::fopen((r.folder + "/__xns.dat").c_str(), "w");
+        if (f) { std::fwrite(xns.data(), 1, xlen, f); std::fclose(f); }
+    }
+    init_energy_file(r);
+    st = cb_create_from_ic(&p, phi0.data(), pi0.data(), &r.line, &r.h);
+    if (st != CB_OK) { std::cerr << "Error: " << cb_last_error(nullptr) << "\n"; return 1; }
+    parameters_file(r);
+    energy_line(r, r.line);
+    if (!snapshot(r, 0)) return 1;
+    if (o.D == 1 && !full_field(r)) return 1;
+
+    const std::vector<int> snaps = schedule(o);
+    size_t next_snap = 0;
+    const int progress = std::max(1, o.nt / 20);
+    int it = 1;
+    while (it <= o.nt) {
+        /* the next step at which something is written */
+        int next = o.nt;
+        next = std::min(next, ((it + kOutEnergyEvery - 1) / kOutEnergyEvery) * kOutEnergyEvery);
+        if (next_snap < snaps.size()) next = std::min(next, snaps[next_snap]);
+        if (o.D == 1) next = std::min(next, ((it + kFull1DFieldEvery - 1) / kFull1DFieldEvery) * kFull1DFieldEvery);
+        next = std::min(next, ((it + progress - 1) / progress) * progress);
+        const bool snap = next_snap < snaps.size() && next == snaps[next_snap];
+        st = cb_step(r.h, next - it + 1, CB_STEP_SUMS | (snap && o.memorysave == 0 ? CB_STEP_LOCAL : 0), &r.line);
+        if (st != CB_OK) return r.fail(st, "stepping") ? 0 : 1;
+        it = next + 1;
+        if (o.D == 1 && next % kFull1DFieldEvery == 0 && !full_field(r)) return 1;
+        if (next % kOutEnergyEvery == 0) energy_line(r, r.line);
+        if (snap) {
+            if (!snapshot(r, (int)++next_snap)) return 1;
+        }
+        if (next % progress == 0)
+            std::cout << "step " << next << " / " << o.nt << " (" << 100 * next / o.nt << "%)" << std::endl;
+    }
+    cb_destroy(r.h);
+    const auto end = std::chrono::high_resolution_clock::now();
+    const double el = std::chrono::duration<double>(end - start).count();
+    std::cout << "Elapsed time: " << el << " seconds\n";
+    FILE *fp = std::fopen((r.folder + "/parameters.dat").c_str(), "a");
+    if (fp) {
+        std::fprintf(fp, "Elapsed time %f seconds\n", el);
+        std::fclose(fp);
+    }
+    return 0;
+}

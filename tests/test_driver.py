@@ -1,0 +1,96 @@
+"""coolbubble_gpu: the reference program's command line and run folder on the
+GPU library. CPU part: option errors and the stability check exit like
+main.cpp (exit code 1). GPU part: a whole run compared file by file with the
+reference executable's own run folder (tests/golden/run_d2, made by
+tests/golden/make_golden.py)."""
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "coolbubble_b200", "lib", "coolbubble_gpu")
+GOLD = os.path.join(ROOT, "tests", "golden", "run_d2")
+
+
+def run(args, cwd=None):
+    return subprocess.run([EXE] + args, capture_output=True, text=True, cwd=cwd, timeout=600)
+
+
+@pytest.mark.parametrize("args,msg", [
+    (["--D", "4"], "--D must be 1, 2 or 3"),
+    (["--nGrids", "1"], "must be positive"),
+    (["--mode", "3"], "--mode must be between -3 and 1"),
+    (["--snapshots", "0"], "--snapshots must be at least 1"),
+    (["--bogus", "1"], "unknown option"),
+    (["--L", "abc"], "cannot read the value"),
+    (["--nt"], "needs a value"),
+])
+def test_bad_options_exit_1(args, msg):
+    r = run(args)
+    assert r.returncode == 1
+    assert msg in r.stderr
+
+
+def test_unstable_time_step_exits_1():
+    r = run(["--D", "2", "--nGrids", "32", "--L", "16", "--dt", "0.4"])
+    assert r.returncode == 1
+    assert "is not satisfied" in r.stdout
+
+
+def _numbers(path, skip_comments=True):
+    rows = []
+    for line in open(path):
+        if skip_comments and line.startswith("#"):
+            continue
+        rows.append([float(x) for x in line.split()])
+    return rows
+
+
+@pytest.mark.gpu
+def test_run_folder_matches_reference_executable():
+    meta = json.load(open(os.path.join(GOLD, "args.json")))
+    with tempfile.TemporaryDirectory() as tmp:
+        r = run(meta["args"] + ["--dt", repr(meta["dt"]), "--out", tmp])
+        assert r.returncode == 0, r.stderr
+        (folder,) = os.listdir(tmp)
+        assert folder == open(os.path.join(GOLD, "folder_name.txt")).read().strip()
+        mine = os.path.join(tmp, folder)
+        names = sorted(os.listdir(GOLD))
+        for fn in names:
+            if fn in ("args.json", "folder_name.txt"):
+                continue
+            a, b = os.path.join(mine, fn), os.path.join(GOLD, fn)
+            assert os.path.exists(a), fn
+            if fn == "__xns.dat":
+                assert open(a).read() == open(b).read()            # bit-exact placement and images
+            elif fn == "parameters.dat":
+                la = [x for x in open(a) if not x.startswith("Elapsed time")]
+                assert la == open(b).readlines()
+            elif fn == "EnergyDensities.dat":
+                A, B = _numbers(a), _numbers(b)
+                assert len(A) == len(B)
+                assert open(a).readlines()[:3] == open(b).readlines()[:3]
+                for ra, rb in zip(A, B):
+                    np.testing.assert_allclose(ra, rb, rtol=2e-9, atol=1e-14)
+            elif fn.startswith("_phi_k_t="):
+                A, B = _numbers(a), _numbers(b)
+                assert len(A) == len(B)
+                for ra, rb in zip(A, B):                            # printed with 6 significant digits
+                    np.testing.assert_allclose(ra, rb, rtol=2e-6, atol=1e-300)
+            elif fn.endswith(".f32"):
+                A, B = np.fromfile(a, dtype=np.float32), np.fromfile(b, dtype=np.float32)
+                assert A.shape == B.shape
+                np.testing.assert_allclose(A, B, rtol=2e-7, atol=1e-12 * max(np.abs(B).max(), 1e-30))
+            elif fn.endswith(".h5"):
+                la, lb = open(a).read().split("\n"), open(b).read().split("\n")
+                assert len(la) == len(lb)
+                for x, y in zip(la, lb):
+                    if x.startswith("attr "):
+                        assert x.split()[1] == y.split()[1]
+                        assert float(x.split()[2]) == pytest.approx(float(y.split()[2]), rel=1e-14, abs=1e-300)
+                    else:
+                        assert x == y
