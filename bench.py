@@ -28,6 +28,11 @@ import time
 
 import numpy as np
 
+# Runs of the serving loop and members of an ensemble each have their own
+# stream; more hardware work queues than the default 8 keep unrelated streams
+# from queueing behind one another. Read when the CUDA context is created.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 

@@ -11,7 +11,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -180,6 +182,44 @@ void fill_sums(const cb_handle *h, const DevState &s, cb_sums *o) {
     o->ekin_half_prev = s.ekin_half_prev;
 }
 
+/* Queue a copy of the run's step record into host memory (pinned, so the copy
+ * is asynchronous); sums_from_record turns it into box averages once it lands. */
+int enqueue_record_copy(cb_handle *h, DevState *dst) {
+    cudaError_t e = cudaMemcpyAsync(dst, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "reading device state");
+    return CB_OK;
+}
+
+int sums_from_record(cb_handle *h, const DevState &s, double t, cb_sums *out) {
+    if (s.err != 0) {
+        char b[128];
+        std::snprintf(b, sizeof b, "a bounded device wait ran out (error word 0x%x); the step did not complete", s.err);
+        return fail(h, CB_ETIMEOUT, b);
+    }
+    if (out) {
+        fill_sums(h, s, out);
+        out->t = t;
+    }
+    return CB_OK;
+}
+
+/* Let the device's default stream-ordered pool keep up to 8 GiB of released
+ * run buffers instead of returning them to the driver at every synchronise, so
+ * a loop that creates and retires runs reuses the same memory. */
+void keep_released_memory() {
+    static std::mutex mu;
+    static std::vector<int> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return; }
+    std::lock_guard<std::mutex> lock(mu);
+    for (int d : done) if (d == dev) return;
+    done.push_back(dev);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) { cudaGetLastError(); return; }
+    uint64_t keep = 8ull << 30;
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) cudaGetLastError();
+}
+
 /* Allocate the device side of a handle (no data yet). */
 int alloc_handle(const cb_params *p, cb_handle **out) {
     std::string why;
@@ -196,11 +236,14 @@ int alloc_handle(const cb_params *p, cb_handle **out) {
     h->N = 1;
     for (int i = 0; i < p->d; ++i) h->N *= (size_t)p->n_grids;
     h->expanding = h->k.expanding != 0;
+    keep_released_memory();
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { int r = cuda_fail(nullptr, e, "creating a stream"); delete h; return r; }
     const size_t bytes = h->N * h->esz;
+    /* stream-ordered allocations: creating and releasing a run never makes the
+     * whole device wait (a serving loop creates and retires runs while others step) */
     auto dalloc = [&](void **ptr, size_t b) -> bool {
-        cudaError_t r = cudaMalloc(ptr, b);
+        cudaError_t r = cudaMallocAsync(ptr, b, h->stream);
         if (r != cudaSuccess) { cudaGetLastError(); *ptr = nullptr; return false; }
         return true;
     };
@@ -223,15 +266,18 @@ int alloc_handle(const cb_params *p, cb_handle **out) {
 
 void destroy_handle(cb_handle *h) {
     if (!h) return;
-    if (h->stream) cudaStreamSynchronize(h->stream);
-    for (int i = 0; i < 2; ++i) { cudaFree(h->phi[i]); cudaFree(h->pi[i]); }
-    for (int i = 0; i < 3; ++i) cudaFree(h->loc[i]);
-    cudaFree(h->partials);
-    cudaFree(h->st);
-    cudaFree(h->tmp);
+    /* every release is ordered after the run's queued work on its own stream */
+    auto dfree = [&](void *p) {
+        if (p) cudaFreeAsync(p, h->stream);
+    };
+    for (int i = 0; i < 2; ++i) { dfree(h->phi[i]); dfree(h->pi[i]); }
+    for (int i = 0; i < 3; ++i) dfree(h->loc[i]);
+    dfree(h->partials);
+    dfree(h->st);
+    dfree(h->tmp);
+    free_fft(h);
     for (int i = 0; i < 2; ++i)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
-    free_fft(h);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -256,8 +302,7 @@ int upload_field(cb_handle *h, void *dst, const double *src) {
 /* Release the staging buffer after the set-up (FP32C uploads need N doubles). */
 void release_tmp(cb_handle *h) {
     if (h->tmp && h->prec == P_FP32) {
-        cudaStreamSynchronize(h->stream);
-        cudaFree(h->tmp);
+        cudaFreeAsync(h->tmp, h->stream);
         h->tmp = nullptr;
         h->tmp_bytes = 0;
     }
@@ -276,10 +321,10 @@ int flush_pending(cb_handle *h) {
 
 int ensure_tmp(cb_handle *h, size_t bytes) {
     if (h->tmp_bytes >= bytes) return CB_OK;
-    cudaFree(h->tmp);
+    if (h->tmp) cudaFreeAsync(h->tmp, h->stream);
     h->tmp = nullptr;
     h->tmp_bytes = 0;
-    cudaError_t e = cudaMalloc(&h->tmp, bytes);
+    cudaError_t e = cudaMallocAsync(&h->tmp, bytes, h->stream);
     if (e != cudaSuccess) { cudaGetLastError(); return fail(h, CB_ENOMEM, "device allocation of a staging buffer failed"); }
     h->tmp_bytes = bytes;
     return CB_OK;

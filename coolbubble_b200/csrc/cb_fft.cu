@@ -333,10 +333,10 @@ bool factor(int n, int *radix, int &ns) {
 
 void free_fft(cb_handle *h) {
     if (!h->fft) return;
-    cudaFree(h->fft->tw);
-    cudaFree(h->fft->half);
-    cudaFree(h->fft->hist);
-    cudaFree(h->fft->bins_out);
+    cudaFreeAsync(h->fft->tw, h->stream);
+    cudaFreeAsync(h->fft->half, h->stream);
+    cudaFreeAsync(h->fft->hist, h->stream);
+    cudaFreeAsync(h->fft->bins_out, h->stream);
     delete h->fft;
     h->fft = nullptr;
 }
@@ -367,15 +367,19 @@ int fft_setup(cb_handle *h, FftState *&out, int d, int n, cudaStream_t s) {
     f->nbins = (int)(std::sqrt(double(d)) * n / 2) + 1;
     f->hist_blocks = 148 * 2;
     std::vector<double2> w = twiddles(n);
-    cudaError_t e = cudaMalloc(&f->tw, n * sizeof(double2));
-    if (e == cudaSuccess) e = cudaMalloc(&f->half, f->half_elems * sizeof(double2));
-    if (e == cudaSuccess) e = cudaMalloc(&f->hist, (size_t)f->hist_blocks * 3 * f->nbins * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&f->bins_out, 3 * (size_t)f->nbins * sizeof(double));
+    cudaError_t e = cudaMallocAsync(&f->tw, n * sizeof(double2), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&f->half, f->half_elems * sizeof(double2), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&f->hist, (size_t)f->hist_blocks * 3 * f->nbins * sizeof(double), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&f->bins_out, 3 * (size_t)f->nbins * sizeof(double), s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(f->tw, w.data(), n * sizeof(double2), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        cudaFree(f->tw); cudaFree(f->half); cudaFree(f->hist); cudaFree(f->bins_out);
+        if (f->tw) cudaFreeAsync(f->tw, s);
+        if (f->half) cudaFreeAsync(f->half, s);
+        if (f->hist) cudaFreeAsync(f->hist, s);
+        if (f->bins_out) cudaFreeAsync(f->bins_out, s);
+        cudaStreamSynchronize(s);
         delete f;
         return fail(h, CB_ENOMEM, std::string("power spectrum buffers: ") + cudaGetErrorString(e));
     }
@@ -508,7 +512,7 @@ int device_c2r(int d, int n, const double *half_host, double *out_dev, cudaStrea
     cudaError_t e = cudaMemcpyAsync(f->half, half_host, f->half_elems * sizeof(double2), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = fft_c2r(f, out_dev, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(f->tw); cudaFree(f->half); cudaFree(f->hist); cudaFree(f->bins_out);
+    cudaFreeAsync(f->tw, s); cudaFreeAsync(f->half, s); cudaFreeAsync(f->hist, s); cudaFreeAsync(f->bins_out, s);
     delete f;
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "inverse DFT");
     return CB_OK;
@@ -534,7 +538,8 @@ extern "C" int cb_dft_c2r(int d, int n, const double *in, double *out) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, dev, N * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(dev);
-    cudaFree(f->tw); cudaFree(f->half); cudaFree(f->hist); cudaFree(f->bins_out);
+    cudaFreeAsync(f->tw, s); cudaFreeAsync(f->half, s); cudaFreeAsync(f->hist, s); cudaFreeAsync(f->bins_out, s);
+    cudaStreamSynchronize(s);
     delete f;
     cudaStreamDestroy(s);
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "cb_dft_c2r");
@@ -560,7 +565,8 @@ extern "C" int cb_dft_r2c(int d, int n, const double *in, double *out) {
         e = cudaMemcpyAsync(out, f->half, f->half_elems * sizeof(double2), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(dev);
-    cudaFree(f->tw); cudaFree(f->half); cudaFree(f->hist); cudaFree(f->bins_out);
+    cudaFreeAsync(f->tw, s); cudaFreeAsync(f->half, s); cudaFreeAsync(f->hist, s); cudaFreeAsync(f->bins_out, s);
+    cudaStreamSynchronize(s);
     delete f;
     cudaStreamDestroy(s);
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "cb_dft_r2c");

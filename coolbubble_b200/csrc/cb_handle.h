@@ -49,6 +49,8 @@ int ensure_tmp(cb_handle *h, size_t bytes);
 void destroy_handle(cb_handle *h);
 void free_fft(cb_handle *h);
 int step_impl(cb_handle *h, int nsteps, int flags, bool timed);
+int enqueue_record_copy(cb_handle *h, DevState *dst);
+int sums_from_record(cb_handle *h, const DevState &s, double t, cb_sums *out);
 int device_c2r(int d, int n, const double *half_host, double *out_dev, cudaStream_t s);
 int device_initial_condition(cb_handle *h, const cb_ic_params *ic, const char *xns_in, std::string *xns_out);
 }  // namespace cb

@@ -123,7 +123,7 @@ int device_initial_condition(cb_handle *h, const cb_ic_params *ic, const char *x
         const double mT = std::sqrt(2 * (c + 6));
         const double T = ic->trad * mT, mF = std::sqrt(2 * c);
         double *tmp = nullptr;
-        e = cudaMalloc(&tmp, N * sizeof(double));
+        e = cudaMallocAsync(&tmp, N * sizeof(double), s);
         if (e != cudaSuccess) { cudaGetLastError(); return fail(h, CB_ENOMEM, "initial condition: staging buffer"); }
         const double norm = 1.0 / std::sqrt(std::pow(L, d));
         for (int which = 0; which < 2; ++which) {
@@ -131,13 +131,13 @@ int device_initial_condition(cb_handle *h, const cb_ic_params *ic, const char *x
             int r = ic_thermal_modes(d, n, L, T, mF, which == 1, ic->thermal_seed,
                                      which == 0 ? "thermalspec" : "velocitythermalspec", half);
             if (r == CB_OK) r = device_c2r(d, n, half.data(), tmp, s);
-            if (r != CB_OK) { cudaFree(tmp); return fail(h, r, "initial condition: inverse DFT"); }
+            if (r != CB_OK) { cudaFreeAsync(tmp, s); return fail(h, r, "initial condition: inverse DFT"); }
             void *dst = which == 0 ? phi : pi;
             if (h->prec == P_FP64) k_scale_into<double><<<grid_for(N), 256, 0, s>>>(tmp, norm, (double *)dst, N);
             else k_scale_into<float><<<grid_for(N), 256, 0, s>>>(tmp, norm, (float *)dst, N);
         }
+        cudaFreeAsync(tmp, s);
         e = cudaStreamSynchronize(s);
-        cudaFree(tmp);
         if (e != cudaSuccess) return cuda_fail(h, e, "initial condition");
         return CB_OK;
     }
@@ -154,9 +154,13 @@ int device_initial_condition(cb_handle *h, const cb_ic_params *ic, const char *x
     double *dxyz = nullptr;
     const int npos = (int)(xyz.size() / 3);
     if (npos > 0) {
-        e = cudaMalloc(&dxyz, xyz.size() * sizeof(double));
+        e = cudaMallocAsync(&dxyz, xyz.size() * sizeof(double), s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(dxyz, xyz.data(), xyz.size() * sizeof(double), cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) { cudaGetLastError(); cudaFree(dxyz); return fail(h, CB_ENOMEM, "initial condition: positions"); }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            if (dxyz) cudaFreeAsync(dxyz, s);
+            return fail(h, CB_ENOMEM, "initial condition: positions");
+        }
     }
     if (h->prec == P_FP64)
         k_ic_profiles<double><<<grid_for(N), 256, 0, s>>>(d, n, L, ic->mode, ic->test, ic->deltar, f, dxyz, npos,
@@ -164,8 +168,8 @@ int device_initial_condition(cb_handle *h, const cb_ic_params *ic, const char *x
     else
         k_ic_profiles<float><<<grid_for(N), 256, 0, s>>>(d, n, L, ic->mode, ic->test, ic->deltar, f, dxyz, npos,
                                                         (float *)phi, N);
+    if (dxyz) cudaFreeAsync(dxyz, s);
     e = cudaStreamSynchronize(s);
-    cudaFree(dxyz);
     if (e != cudaSuccess) return cuda_fail(h, e, "initial condition");
     return CB_OK;
 }

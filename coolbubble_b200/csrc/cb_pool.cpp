@@ -1,15 +1,24 @@
 /* cb_pool.cpp -- a request loop that keeps runs resident on the GPU.
  *
  * No counterpart in the reference (one run per process, main.cpp). Callers
- * submit runs (parameters, initial-condition seed, number of steps); a worker
- * thread admits them against a device-memory budget and a slot limit, builds
- * their initial conditions on the device (cb_create_from_seed), and advances
- * every admitted run concurrently on its own stream in chunks that end at the
- * run's output steps, where it records the box averages. Runs that arrive
- * while others are on the GPU join as soon as a slot and their memory are
- * free (continuous batching); a finished run's memory is released at once.
- * Each run's arithmetic does not depend on the others', so a result is the
- * same alone and in a mix.
+ * submit runs (parameters, initial-condition seed, number of steps). Two
+ * threads serve them:
+ *
+ *  - the admission thread takes runs in arrival order while a slot and their
+ *    memory fit the device-memory budget and builds each start on the device
+ *    (cb_create_from_seed) on the run's own stream, so drawing a start on the
+ *    host never holds up the runs already stepping;
+ *  - the stepping thread keeps every admitted run's stream fed: each run has
+ *    up to RING chunks queued (a chunk ends at the run's next output step and
+ *    is followed by an asynchronous copy of its step record and an event);
+ *    as soon as a run's oldest chunk completes its box averages are taken
+ *    from the record and another chunk is queued. Runs never wait for one
+ *    another, and a finished run's memory goes back to the budget at once
+ *    (released in stream order, without a device-wide synchronise).
+ *
+ * Runs that arrive while others are on the GPU join as soon as a slot and
+ * their memory are free (continuous batching). Each run's arithmetic does not
+ * depend on the others', so a result is the same alone and in a mix.
  */
 #include <algorithm>
 #include <chrono>
@@ -30,6 +39,14 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+constexpr int RING = 2;   /* chunks a run may have queued on its stream */
+
+struct Chunk {
+    int steps = 0;
+    bool report = false;   /* the chunk ends at an output step */
+    double t = 0.0;        /* the run's time after the chunk */
+};
+
 struct Request {
     int64_t id = 0;
     cb_request req{};
@@ -37,9 +54,16 @@ struct Request {
     int state = CB_REQ_QUEUED;
     std::string err;
     cb_handle *h = nullptr;
-    int steps_done = 0;
+    int steps_done = 0;     /* steps whose chunk has completed */
+    int steps_queued = 0;   /* steps queued on the stream */
     int64_t footprint = 0;
     bool cancel = false;
+    bool building = false;  /* the admission thread owns it */
+    int slot = -1;          /* pinned step records and events of the run */
+    Chunk ring[RING];
+    int ring_head = 0, ring_count = 0;
+    int fail_status = CB_OK;
+    std::string fail_why;
     Clock::time_point t_submit, t_admit, t_done;
     std::vector<cb_sums> lines;
     std::vector<float> phi, pi;
@@ -52,8 +76,8 @@ double seconds(Clock::time_point a, Clock::time_point b) { return std::chrono::d
 struct cb_pool {
     std::mutex mu;
     std::condition_variable changed;   /* a request changed state */
-    std::condition_variable work;      /* new work for the worker */
-    std::thread worker;
+    std::condition_variable work;      /* new work for either thread */
+    std::thread admitter, stepper;
     bool stop = false;
     bool broken = false;
     std::string broken_why;
@@ -62,8 +86,12 @@ struct cb_pool {
     int device = 0;
     int64_t next_id = 1;
     std::deque<Request *> queue;
-    std::vector<Request *> active;
+    std::vector<Request *> active;     /* admitted: being built or stepping */
+    std::vector<Request *> ready;      /* built, not yet taken by the stepping thread */
     std::map<int64_t, Request *> all;
+    std::vector<int> free_slots;
+    cb::DevState *records = nullptr;   /* pinned, max_active * RING */
+    std::vector<cudaEvent_t> events;   /* max_active * RING, made by the stepping thread */
     int inject = 0;                    /* test hook: CB_INJECT_* */
     Clock::time_point t0;
     double site_updates = 0.0;
@@ -88,163 +116,261 @@ void finish(cb_pool *P, Request *r, int state, const std::string &why) {
     r->t_done = Clock::now();
     P->used -= r->footprint;
     r->footprint = 0;
+    if (r->slot >= 0) {
+        P->free_slots.push_back(r->slot);
+        r->slot = -1;
+    }
+    auto it = std::find(P->active.begin(), P->active.end(), r);
+    if (it != P->active.end()) P->active.erase(it);
     if (state == CB_REQ_DONE) P->completed++;
     else if (state == CB_REQ_FAILED) P->failed++;
     else if (state == CB_REQ_CANCELLED) P->cancelled++;
     P->changed.notify_all();
+    P->work.notify_all();   /* memory and a slot are free again */
 }
 
-/* Admit from the head of the queue while a slot and the memory are free. */
-void admit(cb_pool *P) {
+/* Called with P->mu held: the head of the queue, if it can be admitted now. */
+Request *admissible_head(cb_pool *P) {
+    while (!P->queue.empty()) {
+        Request *head = P->queue.front();
+        if (head->footprint > P->budget) {
+            P->queue.pop_front();
+            finish(P, head, CB_REQ_FAILED, "run needs more memory than the pool's whole budget");
+            continue;
+        }
+        if ((int)P->active.size() >= P->max_active || P->free_slots.empty()) return nullptr;
+        if (P->used + head->footprint > P->budget) return nullptr;   /* first come, first served */
+        return head;
+    }
+    return nullptr;
+}
+
+void run_admitter(cb_pool *P) {
+    if (cb_set_device(P->device) != CB_OK) {
+        std::lock_guard<std::mutex> lock(P->mu);
+        if (!P->broken) {
+            P->broken = true;
+            P->broken_why = std::string("pool admission stopped: ") + cb_last_error(nullptr);
+        }
+        P->work.notify_all();
+        return;
+    }
     for (;;) {
         Request *r = nullptr;
-        {
-            std::lock_guard<std::mutex> lock(P->mu);
-            if (P->queue.empty() || (int)P->active.size() >= P->max_active) return;
-            Request *head = P->queue.front();
-            if (head->footprint > P->budget) {
-                P->queue.pop_front();
-                finish(P, head, CB_REQ_FAILED, "run needs more memory than the pool's whole budget");
-                continue;
-            }
-            if (P->used + head->footprint > P->budget) return;   /* first come, first served */
-            P->queue.pop_front();
-            P->used += head->footprint;
-            head->state = CB_REQ_RUNNING;
-            head->t_admit = Clock::now();
-            P->admitted++;
-            r = head;
-        }
-        int st = CB_OK;
-        std::string why;
         bool injected = false;
         {
-            std::lock_guard<std::mutex> lock(P->mu);
+            std::unique_lock<std::mutex> lock(P->mu);
+            P->work.wait(lock, [&] { return P->stop || P->broken || admissible_head(P) != nullptr; });
+            if (P->stop || P->broken) return;
+            r = P->queue.front();
+            P->queue.pop_front();
+            P->used += r->footprint;
+            r->state = CB_REQ_RUNNING;
+            r->building = true;
+            r->t_admit = Clock::now();
+            r->slot = P->free_slots.back();
+            P->free_slots.pop_back();
+            P->active.push_back(r);
+            P->admitted++;
             if (P->inject == CB_INJECT_ADMISSION_FAILURE) {
                 P->inject = 0;
                 injected = true;
             }
         }
+        int st = CB_OK;
+        std::string why;
+        cb_handle *h = nullptr;
         if (injected) {
             st = CB_ENOMEM;
             why = "injected admission failure";
         } else {
             cb_sums first;
             st = cb_create_from_seed(&r->req.params, &r->req.ic, r->xns_in.empty() ? nullptr : r->xns_in.c_str(),
-                                     &first, nullptr, 0, nullptr, &r->h);
+                                     &first, nullptr, 0, nullptr, &h);
             if (st != CB_OK) why = cb_last_error(nullptr);
         }
         std::lock_guard<std::mutex> lock(P->mu);
+        r->building = false;
         if (st != CB_OK) {
-            r->h = nullptr;
             finish(P, r, CB_REQ_FAILED, why);
-            continue;
+        } else if (P->broken) {
+            cb_destroy(h);
+            finish(P, r, CB_REQ_FAILED, P->broken_why);
+        } else if (r->cancel) {
+            cb_destroy(h);
+            finish(P, r, CB_REQ_CANCELLED, "cancelled");
+        } else {
+            r->h = h;
+            P->ready.push_back(r);
+            P->work.notify_all();
         }
-        P->active.push_back(r);
     }
 }
 
-/* One tick: every active run advances to its next output step (or its end). */
-void tick(cb_pool *P) {
-    std::vector<Request *> act;
-    {
-        std::lock_guard<std::mutex> lock(P->mu);
-        act = P->active;
+/* Queue the run's next chunk: up to its next output step or its end, then a
+ * copy of its step record and an event. */
+int queue_chunk(cb_pool *P, Request *r) {
+    const int every = r->req.sums_every > 0 ? r->req.sums_every : r->req.nt;
+    const int to_event = every - (r->steps_queued % every);
+    const int k = std::min(to_event, r->req.nt - r->steps_queued);
+    const bool report = r->req.sums_every > 0 && (r->steps_queued + k) % every == 0;
+    int st = cb::step_impl(r->h, k, report ? CB_STEP_SUMS : 0, false);
+    const int at = (r->ring_head + r->ring_count) % RING;
+    const int idx = r->slot * RING + at;
+    if (st == CB_OK) st = cb::enqueue_record_copy(r->h, &P->records[idx]);
+    if (st == CB_OK) {
+        cudaError_t e = cudaEventRecord(P->events[idx], r->h->stream);
+        if (e != cudaSuccess) st = cb::cuda_fail(r->h, e, "recording an event");
     }
-    if (act.empty()) return;
-    {
-        std::lock_guard<std::mutex> lock(P->mu);
-        if (P->inject == CB_INJECT_WORKER_EXCEPTION) {
-            P->inject = 0;
-            throw std::runtime_error("injected worker failure");
-        }
+    if (st != CB_OK) return st;
+    Chunk &c = r->ring[at];
+    c.steps = k;
+    c.report = report;
+    c.t = r->h->t;
+    r->ring_count++;
+    r->steps_queued += k;
+    return CB_OK;
+}
+
+/* Take the run's oldest chunk if it has completed. 1: taken, 0: not yet, <0: failed. */
+int take_chunk(cb_pool *P, Request *r) {
+    const int idx = r->slot * RING + r->ring_head;
+    cudaError_t e = cudaEventQuery(P->events[idx]);
+    if (e == cudaErrorNotReady) return 0;
+    const Chunk c = r->ring[r->ring_head];
+    r->ring_head = (r->ring_head + 1) % RING;
+    r->ring_count--;
+    if (e != cudaSuccess) {
+        r->fail_status = cb::cuda_fail(r->h, e, "running a chunk of steps");
+        r->fail_why = r->h->err;
+        return -1;
     }
-    const auto t_start = Clock::now();
-    std::vector<int> chunk(act.size(), 0);
-    for (size_t i = 0; i < act.size(); ++i) {
-        Request *r = act[i];
-        if (r->cancel) continue;
-        const int every = r->req.sums_every > 0 ? r->req.sums_every : r->req.nt;
-        const int to_event = every - (r->steps_done % every);
-        const int k = std::min(to_event, r->req.nt - r->steps_done);
-        const bool event = (r->steps_done + k) % every == 0 && r->req.sums_every > 0;
-        if (cb::step_impl(r->h, k, event ? CB_STEP_SUMS : 0, false) != CB_OK) {
-            chunk[i] = -1;
-            continue;
-        }
-        chunk[i] = k;
-    }
-    double updates = 0.0;
-    for (size_t i = 0; i < act.size(); ++i) {
-        Request *r = act[i];
-        std::string why;
-        int state = -1;
-        if (r->cancel) {
-            state = CB_REQ_CANCELLED;
-        } else if (chunk[i] < 0) {
-            state = CB_REQ_FAILED;
-            why = r->h->err;
-        } else {
-            const bool event = r->req.sums_every > 0 && (r->steps_done + chunk[i]) % r->req.sums_every == 0;
-            cb_sums line;
-            int st = event ? cb_get_sums(r->h, &line) : cb_sync(r->h);
-            if (st != CB_OK) {
-                state = CB_REQ_FAILED;
-                why = r->h->err;
-            } else {
-                if (event) r->lines.push_back(line);
-                r->steps_done += chunk[i];
-                updates += (double)r->h->N * chunk[i];
-                if (r->steps_done >= r->req.nt) {
-                    if (r->req.want_fields) {
-                        r->phi.resize(r->h->N);
-                        r->pi.resize(r->h->N);
-                        st = cb_get_fields_f32(r->h, r->phi.data(), r->pi.data(), nullptr, nullptr, nullptr);
-                    }
-                    state = st == CB_OK ? CB_REQ_DONE : CB_REQ_FAILED;
-                    if (st != CB_OK) why = r->h->err;
-                }
-            }
-        }
-        if (state >= 0) {
-            cb_destroy(r->h);
-            r->h = nullptr;
-            std::lock_guard<std::mutex> lock(P->mu);
-            P->active.erase(std::find(P->active.begin(), P->active.end(), r));
-            finish(P, r, state, why);
-        }
+    cb_sums line;
+    int st = cb::sums_from_record(r->h, P->records[idx], c.t, c.report ? &line : nullptr);
+    if (st != CB_OK) {
+        r->fail_status = st;
+        r->fail_why = r->h->err;
+        return -1;
     }
     std::lock_guard<std::mutex> lock(P->mu);
-    P->site_updates += updates;
-    P->busy_s += seconds(t_start, Clock::now());
+    if (c.report) r->lines.push_back(line);
+    r->steps_done += c.steps;
+    P->site_updates += (double)r->h->N * c.steps;
+    return 1;
 }
 
-void run_worker(cb_pool *P) {
+void retire(cb_pool *P, Request *r, int state, const std::string &why) {
+    cb_destroy(r->h);   /* stream-ordered releases: no device-wide wait */
+    r->h = nullptr;
+    std::lock_guard<std::mutex> lock(P->mu);
+    finish(P, r, state, why);
+}
+
+void fail_everything(cb_pool *P, std::vector<Request *> &mine, const std::string &why) {
+    std::lock_guard<std::mutex> lock(P->mu);
+    P->broken = true;
+    P->broken_why = why;
+    for (Request *r : P->ready) mine.push_back(r);
+    P->ready.clear();
+    for (Request *r : mine) {
+        if (r->h) cb_destroy(r->h);
+        r->h = nullptr;
+        finish(P, r, CB_REQ_FAILED, why);
+    }
+    mine.clear();
+    for (Request *r : P->queue) finish(P, r, CB_REQ_FAILED, why);
+    P->queue.clear();
+    /* a run the admission thread is still building fails when it returns */
+    P->changed.notify_all();
+    P->work.notify_all();
+}
+
+void run_stepper(cb_pool *P) {
+    std::vector<Request *> mine;
     try {
         if (cb_set_device(P->device) != CB_OK) throw std::runtime_error(cb_last_error(nullptr));
+        for (auto &ev : P->events)
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                throw std::runtime_error("creating the pool's events failed");
+            }
         for (;;) {
             {
                 std::unique_lock<std::mutex> lock(P->mu);
                 if (P->stop) break;
-                if (P->queue.empty() && P->active.empty())
-                    P->work.wait_for(lock, std::chrono::milliseconds(20));
+                if (mine.empty() && P->ready.empty())
+                    P->work.wait_for(lock, std::chrono::milliseconds(20),
+                                     [&] { return P->stop || !P->ready.empty() || P->inject == CB_INJECT_WORKER_EXCEPTION; });
                 if (P->stop) break;
+                for (Request *r : P->ready) mine.push_back(r);
+                P->ready.clear();
+                if (!mine.empty() && P->inject == CB_INJECT_WORKER_EXCEPTION) {
+                    P->inject = 0;
+                    throw std::runtime_error("injected worker failure");
+                }
             }
-            admit(P);
-            tick(P);
+            if (mine.empty()) continue;
+            const auto t_start = Clock::now();
+            bool in_flight = false, progressed = false;
+            for (size_t i = 0; i < mine.size();) {
+                Request *r = mine[i];
+                int got;
+                while (r->ring_count > 0 && (got = take_chunk(P, r)) != 0) {
+                    progressed = true;
+                    if (got < 0) break;
+                }
+                if (r->ring_count > 0 && r->fail_status == CB_OK && !r->cancel) in_flight = true;
+                bool cancel;
+                {
+                    std::lock_guard<std::mutex> lock(P->mu);
+                    cancel = r->cancel;
+                }
+                /* top the run's queue up, unless it is winding down */
+                while (r->fail_status == CB_OK && !cancel && r->ring_count < RING && r->steps_queued < r->req.nt) {
+                    int st = queue_chunk(P, r);
+                    if (st != CB_OK) {
+                        r->fail_status = st;
+                        r->fail_why = r->h->err;
+                    }
+                    progressed = true;
+                    in_flight = true;
+                }
+                int state = -1;
+                std::string why;
+                if (r->ring_count == 0) {
+                    if (r->fail_status != CB_OK) {
+                        state = CB_REQ_FAILED;
+                        why = r->fail_why;
+                    } else if (cancel) {
+                        state = CB_REQ_CANCELLED;
+                        why = "cancelled";
+                    } else if (r->steps_done >= r->req.nt) {
+                        int st = CB_OK;
+                        if (r->req.want_fields) {
+                            r->phi.resize(r->h->N);
+                            r->pi.resize(r->h->N);
+                            st = cb_get_fields_f32(r->h, r->phi.data(), r->pi.data(), nullptr, nullptr, nullptr);
+                        }
+                        state = st == CB_OK ? CB_REQ_DONE : CB_REQ_FAILED;
+                        if (st != CB_OK) why = r->h->err;
+                    }
+                }
+                if (state >= 0) {
+                    retire(P, r, state, why);
+                    mine.erase(mine.begin() + i);
+                    progressed = true;
+                    continue;
+                }
+                ++i;
+            }
+            if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
+            if (in_flight) {
+                std::lock_guard<std::mutex> lock(P->mu);
+                P->busy_s += seconds(t_start, Clock::now());
+            }
         }
     } catch (const std::exception &ex) {
-        std::lock_guard<std::mutex> lock(P->mu);
-        P->broken = true;
-        P->broken_why = std::string("pool worker stopped: ") + ex.what();
-        for (Request *r : P->active) {
-            if (r->h) { cb_destroy(r->h); r->h = nullptr; }
-            finish(P, r, CB_REQ_FAILED, P->broken_why);
-        }
-        P->active.clear();
-        for (Request *r : P->queue) finish(P, r, CB_REQ_FAILED, P->broken_why);
-        P->queue.clear();
-        P->changed.notify_all();
+        fail_everything(P, mine, std::string("pool worker stopped: ") + ex.what());
     }
 }
 
@@ -253,20 +379,29 @@ void run_worker(cb_pool *P) {
 extern "C" {
 
 int cb_pool_create(int64_t budget_bytes, int max_active, cb_pool **out) {
-    if (budget_bytes <= 0 || max_active < 1 || !out) return cb::fail(nullptr, CB_EINVAL, "cb_pool_create: bad arguments");
+    if (budget_bytes <= 0 || max_active < 1 || max_active > 4096 || !out)
+        return cb::fail(nullptr, CB_EINVAL, "cb_pool_create: bad arguments");
     cb_pool *P = new cb_pool();
     P->budget = budget_bytes;
     P->max_active = max_active;
     P->t0 = Clock::now();
     if (cudaGetDevice(&P->device) != cudaSuccess) { cudaGetLastError(); P->device = 0; }
-    P->worker = std::thread(run_worker, P);
+    cudaError_t e = cudaMallocHost(&P->records, (size_t)max_active * RING * sizeof(cb::DevState));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete P;
+        return cb::fail(nullptr, CB_ENOMEM, "cb_pool_create: pinned step records");
+    }
+    P->events.assign((size_t)max_active * RING, nullptr);
+    for (int s = max_active - 1; s >= 0; --s) P->free_slots.push_back(s);
+    P->stepper = std::thread(run_stepper, P);
+    P->admitter = std::thread(run_admitter, P);
     *out = P;
     return CB_OK;
 }
 
 int cb_pool_submit(cb_pool *P, const cb_request *req, const char *xns_in, int64_t *id) {
     if (!P || !req || !id) return cb::fail(nullptr, CB_EINVAL, "cb_pool_submit: bad arguments");
-    std::string why;
     if (req->nt < 1) return cb::fail(nullptr, CB_EINVAL, "cb_pool_submit: nt must be at least 1");
     if (req->sums_every < 0) return cb::fail(nullptr, CB_EINVAL, "cb_pool_submit: sums_every must be >= 0");
     const int64_t fp = footprint_of(req->params);
@@ -285,7 +420,7 @@ int cb_pool_submit(cb_pool *P, const cb_request *req, const char *xns_in, int64_
     P->all[r->id] = r;
     P->queue.push_back(r);
     *id = r->id;
-    P->work.notify_one();
+    P->work.notify_all();
     return CB_OK;
 }
 
@@ -372,7 +507,7 @@ int cb_pool_inject_failure(cb_pool *P, int kind) {
     if (!P || (kind != CB_INJECT_ADMISSION_FAILURE && kind != CB_INJECT_WORKER_EXCEPTION)) return CB_EINVAL;
     std::lock_guard<std::mutex> lock(P->mu);
     P->inject = kind;
-    P->work.notify_one();
+    P->work.notify_all();
     return CB_OK;
 }
 
@@ -383,11 +518,15 @@ int cb_pool_destroy(cb_pool *P) {
         P->stop = true;
         P->work.notify_all();
     }
-    if (P->worker.joinable()) P->worker.join();
+    if (P->admitter.joinable()) P->admitter.join();
+    if (P->stepper.joinable()) P->stepper.join();
     for (auto &kv : P->all) {
         if (kv.second->h) cb_destroy(kv.second->h);
         delete kv.second;
     }
+    for (cudaEvent_t ev : P->events)
+        if (ev) cudaEventDestroy(ev);
+    cudaFreeHost(P->records);
     delete P;
     return CB_OK;
 }
