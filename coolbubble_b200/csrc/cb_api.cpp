@@ -104,10 +104,21 @@ StepConst make_const(const cb_params *p) {
     k.v3 = 2 * cc + 4;
     k.v4 = cc + 3;
     k.dv = p->delta_v;
+    k.c2f = (float)k.c2;
+    k.c3f = (float)k.c3;
+    k.c4f = (float)k.c4;
+    k.v2f = (float)k.v2;
+    k.v3f = (float)k.v3;
+    k.v4f = (float)k.v4;
+    k.dvf = (float)k.dv;
     k.dx = (double)p->L / (double)p->n_grids;   /* bubble.hpp:45 */
     k.dx2 = k.dx * k.dx;
     k.inv_dx2 = 1.0 / k.dx2;
     k.dx2_pow2 = is_pow2_host(k.dx2);
+    k.dtf = (float)k.dt;
+    k.dxf = (float)k.dx;
+    k.dx2f = (float)k.dx2;
+    k.inv_dx2f = (float)k.inv_dx2;
     k.dxLD = std::pow(k.dx / p->L, p->d);       /* bubble.hpp:47 */
     k.mpl = p->mpl;
     k.alpha = p->alpha;

@@ -126,13 +126,13 @@ __global__ void k_ensemble2d(const EnsMember *__restrict__ members, int cs, int 
     }
     cluster.sync();
 
-    const T dt = (T)k.dt;
-    const T inv_dx2 = (T)k.inv_dx2;
-    const T dx2 = (T)k.dx2;
+    const T dt = kc<T>(k.dt, k.dtf);
+    const T inv_dx2 = kc<T>(k.inv_dx2, k.inv_dx2f);
+    const T dx2 = kc<T>(k.dx2, k.dx2f);
     const bool dx2_pow2 = std::is_same<T, float>::value || k.dx2_pow2 != 0;
     const T inv_dx = (T)(1.0 / k.dx);
     const bool dx_pow2 = std::is_same<T, float>::value || (m.dx_pow2 != 0);
-    const T dx = (T)k.dx;
+    const T dx = kc<T>(k.dx, k.dxf);
     const T half = (T)0.5, kin_w = (T)0.5;
     const int up_rank = (rank + 1) % cs, dn_rank = (rank - 1 + cs) % cs;
     const int nvr = n / W;

@@ -51,6 +51,10 @@ struct DevState {
     /* last-block-done ticket and error word */
     unsigned int counter;
     int err;
+    /* work queue of the staged d = 3 step: next item, and blocks finished
+     * (the last block to finish sets both back to zero for the next launch) */
+    unsigned int item_next;
+    unsigned int item_done;
 };
 
 /* Constants of one run, passed by value to every launch. */
@@ -61,6 +65,10 @@ struct StepConst {
     double dt;
     double c2, c3, c4;  /* V'(f) = c2 f - c3 f^2 + c4 f^3, coefficients as bubble.cpp:76 forms them */
     double v2, v3, v4, dv; /* V(f) = v2 f^2 - v3 f^3 + v4 f^4 + DeltaV (bubble.cpp:71) */
+    /* the same coefficients rounded to float once on the host, so float kernels
+     * read them straight from the parameter bank instead of converting per site */
+    float c2f, c3f, c4f, v2f, v3f, v4f, dvf;
+    float dtf, dxf, dx2f, inv_dx2f;
     double dx, dx2, inv_dx2;
     int dx2_pow2;
     double dxLD, mpl;
@@ -82,6 +90,7 @@ size_t step_blocks(const StepConst &k);
 
 /* d = 3 kernel with TMA-staged row tiles (cb_step3.cu). */
 bool step3_geometry(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid);
+size_t step3_partial_rows(const StepConst &k, int prec);
 cudaError_t launch_step3(int prec, const StepConst &k, bool drift_first, int sums, const void *phi_in,
                          const void *pi_in, void *phi_out, void *pi_out, void *loc_ek, void *loc_eg, void *loc_ep,
                          DevState *st, double *partials, cudaStream_t s);

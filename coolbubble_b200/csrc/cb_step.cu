@@ -76,8 +76,8 @@ __global__ void __launch_bounds__(TX *TY) k_step(StepConst k, const T *__restric
     /* float: multiply by the reciprocal; double: divide unless the divisor is a power of two (exact) */
     const bool adx_pow2 = std::is_same<T, float>::value || st->adx_pow2 != 0;
     const T p = DF ? (T)st->drift_p : (T)1;
-    const T dt = (T)k.dt;
-    const T dx2 = (T)k.dx2, inv_dx2 = (T)k.inv_dx2;
+    const T dt = kc<T>(k.dt, k.dtf);
+    const T dx2 = kc<T>(k.dx2, k.dx2f), inv_dx2 = kc<T>(k.inv_dx2, k.inv_dx2f);
     const bool dx2_pow2 = std::is_same<T, float>::value || k.dx2_pow2 != 0;
     const T half = (T)0.5;
 
@@ -181,8 +181,9 @@ __global__ void __launch_bounds__(TX *TY) k_step(StepConst k, const T *__restric
 #pragma unroll
         for (int s = 0; s < NSUM; ++s) v[s] = acc[s].value();
         __shared__ double tot[NSUM];
-        if (reduce_last_block<TX * TY>(v, partials, &st->counter, tot)) {
-            if (threadIdx.x == 0 && threadIdx.y == 0) epilogue(k, st, tot, !DF, SUMS == SUM_FULL);
+        if (reduce_last_block<TX * TY, SUMS == SUM_FULL ? NSUM : 3>(v, partials, &st->counter, tot)) {
+            const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+            if (tid < 32) epilogue(k, st, tot, !DF, SUMS == SUM_FULL, tid);
         }
     }
 }
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(NT) k_ic_backkick(StepConst k, size_t N, const
             lap = ax == 0 ? t : A::add(lap, t);
         }
         const T flap = A::mul(fl, lap);
-        const T force = A::sub(k.dx2_pow2 ? A::mul(flap, (T)k.inv_dx2) : A::div(flap, (T)k.dx2),
+        const T force = A::sub(k.dx2_pow2 ? A::mul(flap, kc<T>(k.inv_dx2, k.inv_dx2f)) : A::div(flap, kc<T>(k.dx2, k.dx2f)),
                                A::mul(fv, dV<T>(k, f)));
         const T pv = A::sub(pi[s], A::mul(hdt, force));
         pi[s] = pv;
@@ -381,7 +382,7 @@ size_t step_blocks(const StepConst &k) {
         int tj, ns;
         size_t sm;
         unsigned g3;
-        if (step3_geometry(k, prec, tj, ns, sm, g3) && g3 > b) b = g3;
+        if (step3_geometry(k, prec, tj, ns, sm, g3)) b = std::max(b, step3_partial_rows(k, prec));
     }
     return b;
 }

@@ -4,25 +4,32 @@
  * Bubble::oneStep, reference src/bubble.cpp:849-876), organised for HBM
  * bandwidth on the 3-D lattices that dominate run time:
  *
- *  - A work item is a tile of TJ full rows (all n sites of axis 2) of axis 1,
- *    marched over a chunk of CZ planes of axis 0. Full rows make the axis-2
- *    neighbours wrap inside shared memory: no column halo, no wrap logic.
+ *  - A tile is TJ full rows (all n sites of axis 2) of axis 1. Full rows make
+ *    the axis-2 neighbours wrap inside shared memory: no column halo, no wrap
+ *    logic. A work item is one tile over a part of the planes of axis 0.
  *  - Plane p of the tile -- TJ rows of phi, the two periodic halo rows
  *    (j0 - 1) mod n and (j0 + TJ) mod n, and TJ rows of pi (TJ + 2 for the
  *    drift-first ordering) -- arrives by TMA bulk copies (cp.async.bulk,
  *    contiguous rows) into one stage of an S-deep shared-memory ring and
- *    completes an mbarrier with its byte count. One thread issues the copies
- *    S - 3 planes ahead of the plane being computed, so every block keeps
- *    several planes in flight.
+ *    completes an mbarrier with its byte count. One producer thread issues
+ *    the copies as stages free up, so every block keeps several planes in
+ *    flight, and the ring runs on from one item to the next.
+ *  - The grid is one block per resident slot (2 per SM); blocks take items
+ *    from a device-wide queue. Each item's box sums go to its own row of
+ *    partial sums, so the totals do not depend on which block took it.
  *  - Each thread updates 16-byte vectors (4 floats / 2 doubles) and stores
  *    phi and pi with 128-bit coalesced writes.
+ *  - Drift-first (expanding background): the pending drift of the previous
+ *    step is applied once to each plane in shared memory as it lands.
  *  - Every mbarrier wait is bounded (clock64 limit): on timeout the block
  *    records an error word in the device state, waits (bounded) for its own
- *    copies still in flight, and returns.
+ *    copies still in flight, and returns; consumer warps that share a
+ *    barrier leave together (a vote in the barrier).
  */
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <type_traits>
 
 #include "cb_internal.h"
@@ -36,10 +43,25 @@ namespace {
 constexpr int CW = 8;                 /* consumer warps */
 constexpr int NC = CW * 32;           /* consumer threads */
 constexpr int NT3 = NC + 32;          /* plus one producer warp */
-constexpr int HDR = 256;              /* full[16] and empty[16] mbarriers */
+constexpr int HDR = 256;              /* full[8], empty[8] and item_full[IQ] mbarriers */
+constexpr int IQ = 8;                 /* items the producer may hand over ahead of the consumers */
 
 /* barrier among the consumer warps only (id 1; id 0 is __syncthreads) */
-__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(NC) : "memory"); }
+__device__ __forceinline__ void consumer_bar() { asm volatile("bar.sync 1, %0;" ::"n"(NC) : "memory"); }
+
+/* the same barrier, also returning whether any consumer thread passed true */
+__device__ __forceinline__ bool consumer_any(bool x) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, 1, %2, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)x), "n"(NC)
+        : "memory");
+    return r != 0;
+}
 
 /* Shared-memory layout of one stage: phi rows [TJ + 2][n] (row 0 and TJ + 1
  * are the halo rows), then pi rows [TJ + 2*DF][n] (drift-first also needs the
@@ -53,41 +75,52 @@ struct StageGeom {
 };
 
 template <typename T, bool DF, int SUMS>
-__global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstage, int cz, const T *__restrict__ phi_in,
-                                                const T *__restrict__ pi_in, T *__restrict__ phi_out,
-                                                T *__restrict__ pi_out, T *__restrict__ loc_ek,
-                                                T *__restrict__ loc_eg, T *__restrict__ loc_ep, DevState *st,
-                                                double *partials) {
+__global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstage, int parts,
+                                                const T *__restrict__ phi_in, const T *__restrict__ pi_in,
+                                                T *__restrict__ phi_out, T *__restrict__ pi_out,
+                                                T *__restrict__ loc_ek, T *__restrict__ loc_eg,
+                                                T *__restrict__ loc_ep, DevState *st, double *partials) {
     using A = Ar<T>;
     using VT = typename Vec<T>::V;
     constexpr int W = Vec<T>::W;
+    constexpr bool UNI = DF || SUMS != SUM_NONE;       /* consumers leave together */
+    constexpr int NS = SUMS == SUM_FULL ? NSUM : 3;    /* sums carried (S_EK, S_EP, S_EG first) */
     extern __shared__ __align__(128) unsigned char smraw[];
     const int n = k.n;
     const StageGeom<T, DF> g{n, tj};
     const size_t stage_elems = g.elems();
     uint64_t *full = reinterpret_cast<uint64_t *>(smraw);
-    uint64_t *empty = full + 16;
+    uint64_t *empty = full + 8;
+    uint64_t *item_full = full + 16;
     T *ring = reinterpret_cast<T *>(smraw + HDR);
     __shared__ int abort_flag;
     __shared__ int issued_count;
+    __shared__ int item_q[IQ];
+    __shared__ double item_red[2][CW][NS];
 
     const int ntiles = n / tj;
-    const int tile = blockIdx.x % ntiles;
-    const int chunk = blockIdx.x / ntiles;
-    const int j0 = tile * tj;
-    const int i0 = chunk * cz;
-    const int i1 = min(i0 + cz, n);
+    /* Work items: (plane part, tile), part-major with tiles fastest; part c
+     * covers planes [c n / parts, (c + 1) n / parts). Blocks take items from a
+     * device-wide queue (an atomic counter in the device state), so the items
+     * in flight are neighbouring tiles of the same planes (their halo rows
+     * meet in L2) and faster SMs simply take more items. An item computing
+     * planes [p0, p1) streams planes p0 - 1 .. p1 through the ring. Ring
+     * positions q count the planes a block streams over all its items; the
+     * producer hands each item to the consumers through a small shared queue
+     * guarded by its own mbarriers. */
+    const int items = ntiles * parts;
     const size_t row_bytes = (size_t)n * sizeof(T);
     const size_t plane = (size_t)n * n;
-    const int jm = (j0 - 1 + n) % n, jp = (j0 + tj) % n;
     const uint32_t tx_bytes = (uint32_t)(((size_t)(tj + 2) + g.pi_rows()) * row_bytes);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-    /* planes needed: i0 - 1 .. i1 (the axis-0 neighbours of the chunk) */
-    const int first = i0 - 1;
-    const int count = i1 - i0 + 2;
-    auto stage_of = [&](int p) { return (p - first) % nstage; };
-    auto parity_of = [&](int p) { return (uint32_t)(((p - first) / nstage) & 1); };
+    auto stage_of = [&](int q) { return q % nstage; };
+    auto parity_of = [&](int q) { return (uint32_t)((q / nstage) & 1); };
+    auto item_of = [&](int it, int &t, int &p0, int &p1) {
+        const int c = it / ntiles;
+        t = it % ntiles;
+        p0 = (int)((long long)c * n / parts);
+        p1 = (int)((long long)(c + 1) * n / parts);
+    };
 
     if (threadIdx.x == 0) {
         abort_flag = 0;
@@ -96,6 +129,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], CW);
         }
+        for (int s = 0; s < IQ; ++s) mbar_init(&item_full[s], 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -103,11 +137,13 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
     Acc<T> acc[NSUM];
 
     if (warp == CW) {
-        /* ---- producer warp: lane 0 issues the bulk copies of every plane,
-         *      reusing a stage once all consumer warps released the plane it held ---- */
-        auto issue = [&](int q) {
+        /* ---- producer warp: lane 0 takes items from the queue and issues the
+         *      bulk copies of their planes, reusing a stage once all consumer
+         *      warps released the plane it held ---- */
+        auto issue = [&](int q, int pl, int j0) {
             const int s = q % nstage;
-            const int pw = (first + q + n) % n;
+            const int pw = (pl + n) % n;
+            const int jm = (j0 - 1 + n) % n, jp = (j0 + tj) % n;
             T *dst = ring + (size_t)s * stage_elems;
             const T *src_phi = phi_in + (size_t)pw * plane;
             const T *src_pi = pi_in + (size_t)pw * plane;
@@ -125,17 +161,41 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                 bulk_g2s(dpi, src_pi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
             }
         };
-        /* stage reuse: plane q goes where plane q - nstage was, once released */
+        /* stage reuse: position q goes where position q - nstage was, once released */
         auto free_for = [&](int q) -> bool {
             const int use = q / nstage;
             return use == 0 || mbar_wait(&empty[q % nstage], (uint32_t)((use - 1) & 1), WAIT_LIMIT);
         };
         if (lane == 0) {
             int q = 0;
-            for (; q < count; ++q) {
-                if (!free_for(q)) { atomicExch(&abort_flag, 1); break; }
-                if (abort_flag) break;
-                issue(q);
+            bool ok = true;
+            int cur = (int)atomicAdd(&st->item_next, 1u);
+            for (int j = 0; ok; ++j) {
+                /* hand item j (or the end of the queue) to the consumers; the
+                 * queue slot was read IQ items ago: every item streams at least
+                 * three planes and the ring holds at most six, so the producer
+                 * stays within three items of the consumers */
+                item_q[j % IQ] = cur < items ? cur : -1;
+                mbar_arrive(&item_full[j % IQ]);
+                if (cur >= items) break;
+                int t, p0, p1;
+                item_of(cur, t, p0, p1);
+                for (int pl = p0 - 1; pl <= p1; ++pl, ++q) {
+                    if (!free_for(q)) {
+                        atomicExch(&abort_flag, 1);
+                        ok = false;
+                        break;
+                    }
+                    if (abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    issue(q, pl, t * tj);
+                }
+                /* the next item is taken only now, with this one fully issued:
+                 * taken earlier, a block would hold back an item an idle block
+                 * could run (the consumers still have the ring's planes to do) */
+                if (ok) cur = (int)atomicAdd(&st->item_next, 1u);
             }
             issued_count = q;
         }
@@ -145,166 +205,295 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         const T adx = (T)st->adx, inv_adx = (T)st->inv_adx;
         /* float: multiply by the reciprocal; double: divide unless the divisor is a power of two (exact) */
         const bool adx_pow2 = std::is_same<T, float>::value || st->adx_pow2 != 0;
-        const T dt = (T)k.dt;
+        const T dt = kc<T>(k.dt, k.dtf);
         const T p = DF ? (T)st->drift_p : (T)1;
-        const T dx2 = (T)k.dx2, inv_dx2 = (T)k.inv_dx2;
+        const T dx2 = kc<T>(k.dx2, k.dx2f), inv_dx2 = kc<T>(k.inv_dx2, k.inv_dx2f);
         const bool dx2_pow2 = std::is_same<T, float>::value || k.dx2_pow2 != 0;
         const T half = (T)0.5;
         auto grad = [&](T dphi) -> T { return adx_pow2 ? A::mul(dphi, inv_adx) : A::div(dphi, adx); };
         const int nvec_row = n / W;
         const int nvec = tj * nvec_row;
-        /* wait for plane pl to land */
-        auto acquire = [&](int pl) -> bool {
-            uint64_t *bar = &full[stage_of(pl)];
-            const bool ok = abort_flag == 0 && mbar_wait(bar, parity_of(pl), WAIT_LIMIT);
+        const int row_step = NC / nvec_row, vec_step = NC % nvec_row;
+        const bool want_eg = SUMS == SUM_FULL || k.alpha == 1;
+        /* wait for ring position q to land */
+        auto acquire = [&](int q) -> bool {
+            const bool ok = abort_flag == 0 && mbar_wait(&full[stage_of(q)], parity_of(q), WAIT_LIMIT);
             if (!ok) atomicExch(&abort_flag, 1);
             return ok;
         };
-        bool run = acquire(first) && acquire(first + 1);
-        for (int i = i0; run && i < i1; ++i) {
-            if (!acquire(i + 1)) break;
-            const T *Sm = ring + (size_t)stage_of(i - 1) * stage_elems;
-            const T *S0 = ring + (size_t)stage_of(i) * stage_elems;
-            const T *Sp = ring + (size_t)stage_of(i + 1) * stage_elems;
-            const T *P0 = S0 + g.phi_elems() + (DF ? n : 0);
-            const size_t gbase = ((size_t)i * n + j0) * n;
-            for (int v = threadIdx.x; v < nvec; v += NC) {
-                const int r = v / nvec_row, kv = v % nvec_row;
-                const int kk = kv * W;
-                const size_t c_off = (size_t)(r + 1) * n + kk;
-                VT c = *reinterpret_cast<const VT *>(S0 + c_off);
-                VT um = *reinterpret_cast<const VT *>(S0 + c_off - n);
-                VT up = *reinterpret_cast<const VT *>(S0 + c_off + n);
-                VT im = *reinterpret_cast<const VT *>(Sm + c_off);
-                VT ip = *reinterpret_cast<const VT *>(Sp + c_off);
-                const VT pv = *reinterpret_cast<const VT *>(P0 + (size_t)r * n + kk);
-                const size_t lo = (size_t)(r + 1) * n + (kk == 0 ? n - 1 : kk - 1);
-                const size_t ro = (size_t)(r + 1) * n + (kk + W == n ? 0 : kk + W);
-                T left = S0[lo];
-                T right = S0[ro];
-                if (DF) {
-                    /* the pending drift phi += (dt pi) p of the previous step (bubble.cpp:867-870),
-                     * applied to every value read; the pi stage rows line up with the phi rows */
-                    const size_t po = g.phi_elems();
-                    auto drift_v = [&](VT &f, const T *base, size_t off) {
-                        const VT v = *reinterpret_cast<const VT *>(base + po + off);
+        /* drift-first: the pending drift phi += (dt pi) p of the previous step
+         * (bubble.cpp:867-870) is applied once to each plane as it lands, in
+         * place, to all its rows (halo rows included: the pi stage rows line up
+         * with the phi rows); every later read then sees the drifted field */
+        auto drift_plane = [&](int q) {
+            T *S = ring + (size_t)stage_of(q) * stage_elems;
+            const T *Pi = S + g.phi_elems();
+            const int nv = (tj + 2) * n / W;
+            for (int v = threadIdx.x; v < nv; v += NC) {
+                VT f = *reinterpret_cast<const VT *>(S + (size_t)v * W);
+                const VT mom = *reinterpret_cast<const VT *>(Pi + (size_t)v * W);
 #pragma unroll
-                        for (int t = 0; t < W; ++t)
-                            Vec<T>::set(f, t, A::add(Vec<T>::get(f, t), A::mul(A::mul(dt, Vec<T>::get(v, t)), p)));
-                    };
-                    drift_v(c, S0, c_off);
-                    drift_v(um, S0, c_off - n);
-                    drift_v(up, S0, c_off + n);
-                    drift_v(im, Sm, c_off);
-                    drift_v(ip, Sp, c_off);
-                    left = A::add(left, A::mul(A::mul(dt, S0[po + lo]), p));
-                    right = A::add(right, A::mul(A::mul(dt, S0[po + ro]), p));
+                for (int t = 0; t < W; ++t)
+                    Vec<T>::set(f, t, A::add(Vec<T>::get(f, t), A::mul(A::mul(dt, Vec<T>::get(mom, t)), p)));
+                *reinterpret_cast<VT *>(S + (size_t)v * W) = f;
+            }
+        };
+        /* drift-first and the sums run consumer barriers (per plane, per item):
+         * every consumer warp then takes the same exit (a vote in the barrier)
+         * when a wait runs out */
+        bool run = true;
+        int qs = 0;   /* ring position of the item's first plane */
+        for (int j = 0; run; ++j) {
+            if (abort_flag != 0 || !mbar_wait(&item_full[j % IQ], (uint32_t)((j / IQ) & 1), WAIT_LIMIT)) {
+                atomicExch(&abort_flag, 1);
+                run = false;
+            }
+            if (UNI) {
+                if (consumer_any(!run)) {
+                    run = false;
+                    break;
                 }
-                VT phi_new, pi_new, vek, veg, vep;
+            } else if (!run) {
+                break;
+            }
+            const int it = item_q[j % IQ];
+            if (it < 0) break;
+            int t, p0, p1;
+            item_of(it, t, p0, p1);
+            const int j0 = t * tj;
+            const int len = p1 - p0 + 2;
+            if (SUMS != SUM_NONE) {
 #pragma unroll
-                for (int s = 0; s < W; ++s) {
-                    const T cur = Vec<T>::get(c, s);
-                    const T kmn = s == 0 ? left : Vec<T>::get(c, s - 1);
-                    const T kpl = s == W - 1 ? right : Vec<T>::get(c, s + 1);
-                    const T two = A::add(cur, cur);
-                    const T nxt = Vec<T>::get(ip, s);
-                    /* Laplacian, axes 0, 1, 2 in the reference's order (bubble.cpp:731-736) */
-                    const T t0 = A::add(A::sub(nxt, two), Vec<T>::get(im, s));
-                    const T t1 = A::add(A::sub(Vec<T>::get(up, s), two), Vec<T>::get(um, s));
-                    const T t2 = A::add(A::sub(kpl, two), kmn);
-                    const T lap = A::add(A::add(t0, t1), t2);
-                    const T flap = A::mul(fl, lap);
-                    const T force =
-                        A::sub(dx2_pow2 ? A::mul(flap, inv_dx2) : A::div(flap, dx2), A::mul(fv, dV<T>(k, cur)));
-                    const T pic = Vec<T>::get(pv, s);
-                    const T pn = A::add(pic, A::mul(dt, force));
-                    Vec<T>::set(pi_new, s, pn);
-                    Vec<T>::set(phi_new, s, DF ? cur : A::add(cur, A::mul(dt, pn)));
-                    if (SUMS != SUM_NONE) {
-                        T eg = (T)0;
-                        if (SUMS == SUM_FULL || k.alpha == 1) {
-                            /* forward gradients: x <- axis 1, y <- axis 0, z <- axis 2 (bubble.cpp:794-801) */
-                            const T gx = grad(A::sub(Vec<T>::get(up, s), cur));
-                            const T gy = grad(A::sub(nxt, cur));
-                            const T gz = grad(A::sub(kpl, cur));
-                            eg = A::mul(half, A::add(A::add(A::sq(gx), A::sq(gy)), A::sq(gz)));
-                        }
-                        const T ep = Vpot<T>(k, cur);
-                        const T ek = A::mul(A::mul(kin_w, pn), pn);
-                        acc[S_EK].add(ek);
-                        acc[S_EP].add(ep);
-                        acc[S_EG].add(eg);
-                        if (SUMS == SUM_FULL) {
-                            const T vv = A::mul(pn, vel_w);
-                            const T et = A::add(A::add(ek, eg), ep);
-                            acc[S_PHI].add(cur);
-                            acc[S_V].add(vv);
-                            acc[Q_EK].add(A::sq(ek));
-                            acc[Q_EP].add(A::sq(ep));
-                            acc[Q_EG].add(A::sq(eg));
-                            acc[Q_ET].add(A::sq(et));
-                            acc[Q_PHI].add(A::sq(cur));
-                            acc[Q_V].add(A::sq(vv));
-                            acc[S_EKIN_IN].add(A::mul(A::mul(kin_w, pic), pic));
-                            Vec<T>::set(vek, s, ek);
-                            Vec<T>::set(veg, s, eg);
-                            Vec<T>::set(vep, s, ep);
+                for (int s = 0; s < NSUM; ++s) acc[s] = Acc<T>{};
+            }
+            bool ok = acquire(qs) && acquire(qs + 1);
+            if (UNI) {
+                if (DF && ok) {
+                    drift_plane(qs);
+                    drift_plane(qs + 1);
+                }
+                if (consumer_any(!ok)) { run = false; break; }
+            } else if (!ok) {
+                run = false;
+                break;
+            }
+            for (int i = p0; i < p1; ++i) {
+                const int qi = qs + (i - p0) + 1;   /* position of plane i */
+                ok = acquire(qi + 1);
+                if (UNI) {
+                    if (DF && ok) drift_plane(qi + 1);
+                    if (consumer_any(!ok)) { run = false; break; }
+                } else if (!ok) {
+                    run = false;
+                    break;
+                }
+                const T *Sm = ring + (size_t)stage_of(qi - 1) * stage_elems;
+                const T *S0 = ring + (size_t)stage_of(qi) * stage_elems;
+                const T *Sp = ring + (size_t)stage_of(qi + 1) * stage_elems;
+                const T *P0 = S0 + g.phi_elems() + (DF ? n : 0);
+                const size_t gbase = ((size_t)i * n + j0) * n;
+                /* (row, vector) of v, stepped by NC without a division per vector */
+                int r = threadIdx.x / nvec_row, kv = threadIdx.x % nvec_row;
+                for (int v = threadIdx.x; v < nvec; v += NC, r += row_step, kv += vec_step) {
+                    if (kv >= nvec_row) {
+                        kv -= nvec_row;
+                        ++r;
+                    }
+                    const int kk = kv * W;
+                    const size_t c_off = (size_t)(r + 1) * n + kk;
+                    const VT c = *reinterpret_cast<const VT *>(S0 + c_off);
+                    const VT um = *reinterpret_cast<const VT *>(S0 + c_off - n);
+                    const VT up = *reinterpret_cast<const VT *>(S0 + c_off + n);
+                    const VT im = *reinterpret_cast<const VT *>(Sm + c_off);
+                    const VT ip = *reinterpret_cast<const VT *>(Sp + c_off);
+                    const VT pv = *reinterpret_cast<const VT *>(P0 + (size_t)r * n + kk);
+                    const size_t lo = (size_t)(r + 1) * n + (kk == 0 ? n - 1 : kk - 1);
+                    const size_t ro = (size_t)(r + 1) * n + (kk + W == n ? 0 : kk + W);
+                    const T left = S0[lo];
+                    const T right = S0[ro];
+                    VT phi_new, pi_new, vek, veg, vep;
+                    /* float: the sites of a vector are summed plainly (W terms), then
+                     * the vector's sum enters the compensated per-thread accumulator;
+                     * double: every site enters the accumulator in site order */
+                    T part[NSUM];
+#pragma unroll
+                    for (int s = 0; s < NSUM; ++s) part[s] = (T)0;
+                    auto put = [&](int s, T x) {
+                        if constexpr (std::is_same<T, float>::value) part[s] = A::add(part[s], x);
+                        else acc[s].add(x);
+                    };
+#pragma unroll
+                    for (int s = 0; s < W; ++s) {
+                        const T cur = Vec<T>::get(c, s);
+                        const T kmn = s == 0 ? left : Vec<T>::get(c, s - 1);
+                        const T kpl = s == W - 1 ? right : Vec<T>::get(c, s + 1);
+                        const T two = A::add(cur, cur);
+                        const T nxt = Vec<T>::get(ip, s);
+                        /* Laplacian, axes 0, 1, 2 in the reference's order (bubble.cpp:731-736) */
+                        const T t0 = A::add(A::sub(nxt, two), Vec<T>::get(im, s));
+                        const T t1 = A::add(A::sub(Vec<T>::get(up, s), two), Vec<T>::get(um, s));
+                        const T t2 = A::add(A::sub(kpl, two), kmn);
+                        const T lap = A::add(A::add(t0, t1), t2);
+                        const T flap = A::mul(fl, lap);
+                        const T force =
+                            A::sub(dx2_pow2 ? A::mul(flap, inv_dx2) : A::div(flap, dx2), A::mul(fv, dV<T>(k, cur)));
+                        const T pic = Vec<T>::get(pv, s);
+                        const T pn = A::add(pic, A::mul(dt, force));
+                        Vec<T>::set(pi_new, s, pn);
+                        Vec<T>::set(phi_new, s, DF ? cur : A::add(cur, A::mul(dt, pn)));
+                        if (SUMS != SUM_NONE) {
+                            T eg = (T)0;
+                            if (want_eg) {
+                                /* forward gradients: x <- axis 1, y <- axis 0, z <- axis 2 (bubble.cpp:794-801) */
+                                const T gx = grad(A::sub(Vec<T>::get(up, s), cur));
+                                const T gy = grad(A::sub(nxt, cur));
+                                const T gz = grad(A::sub(kpl, cur));
+                                eg = A::mul(half, A::add(A::add(A::sq(gx), A::sq(gy)), A::sq(gz)));
+                            }
+                            const T ep = Vpot<T>(k, cur);
+                            const T ek = A::mul(A::mul(kin_w, pn), pn);
+                            put(S_EK, ek);
+                            put(S_EP, ep);
+                            if (want_eg) put(S_EG, eg);
+                            if (SUMS == SUM_FULL) {
+                                const T vv = A::mul(pn, vel_w);
+                                const T et = A::add(A::add(ek, eg), ep);
+                                put(S_PHI, cur);
+                                put(S_V, vv);
+                                put(Q_EK, A::sq(ek));
+                                put(Q_EP, A::sq(ep));
+                                put(Q_EG, A::sq(eg));
+                                put(Q_ET, A::sq(et));
+                                put(Q_PHI, A::sq(cur));
+                                put(Q_V, A::sq(vv));
+                                put(S_EKIN_IN, A::mul(A::mul(kin_w, pic), pic));
+                                Vec<T>::set(vek, s, ek);
+                                Vec<T>::set(veg, s, eg);
+                                Vec<T>::set(vep, s, ep);
+                            }
                         }
                     }
+                    if constexpr (std::is_same<T, float>::value) {
+                        if (SUMS != SUM_NONE) {
+                            acc[S_EK].add(part[S_EK]);
+                            acc[S_EP].add(part[S_EP]);
+                            if (want_eg) acc[S_EG].add(part[S_EG]);
+                        }
+                        if (SUMS == SUM_FULL) {
+#pragma unroll
+                            for (int s = 0; s < NSUM; ++s)
+                                if (s != S_EK && s != S_EP && s != S_EG) acc[s].add(part[s]);
+                        }
+                    }
+                    const size_t o = gbase + (size_t)r * n + kk;
+                    *reinterpret_cast<VT *>(pi_out + o) = pi_new;
+                    *reinterpret_cast<VT *>(phi_out + o) = phi_new;
+                    if (SUMS == SUM_FULL && k.want_local) {
+                        *reinterpret_cast<VT *>(loc_ek + o) = vek;
+                        *reinterpret_cast<VT *>(loc_eg + o) = veg;
+                        *reinterpret_cast<VT *>(loc_ep + o) = vep;
+                    }
                 }
-                const size_t o = gbase + (size_t)r * n + kk;
-                *reinterpret_cast<VT *>(pi_out + o) = pi_new;
-                *reinterpret_cast<VT *>(phi_out + o) = phi_new;
-                if (SUMS == SUM_FULL && k.want_local) {
-                    *reinterpret_cast<VT *>(loc_ek + o) = vek;
-                    *reinterpret_cast<VT *>(loc_eg + o) = veg;
-                    *reinterpret_cast<VT *>(loc_ep + o) = vep;
+                /* this warp no longer needs plane i - 1; with drift-first the plane was
+                 * also written through the generic proxy, so order those writes before
+                 * the copy that will refill the stage */
+                if (DF) fence_proxy_async();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[stage_of(qi - 1)]);
+            }
+            if (!run) break;
+            if (SUMS != SUM_NONE) {
+                /* the item's sums: per warp by shuffle, then warp 0 adds the warps
+                 * in order into the item's own row of partials (fixed place, fixed
+                 * order: independent of which block took the item). The rows are
+                 * double-buffered by item parity: a warp writes the next item's
+                 * values only after the next barrier, which warp 0 reaches after
+                 * reading these. */
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    double x = acc[s].value();
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));
+                    if (lane == 0) item_red[j & 1][warp][s] = x;
+                }
+                consumer_bar();
+                if (warp == 0 && lane < NS) {
+                    double x = 0.0;
+#pragma unroll
+                    for (int w = 0; w < CW; ++w) x = __dadd_rn(x, item_red[j & 1][w][lane]);
+                    partials[(size_t)it * NSUM + lane] = x;
                 }
             }
-            /* this warp no longer needs plane i - 1 */
+            /* the item's last two planes */
+            if (DF) fence_proxy_async();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[stage_of(i - 1)]);
+            if (lane == 0) {
+                mbar_arrive(&empty[stage_of(qs + len - 2)]);
+                mbar_arrive(&empty[stage_of(qs + len - 1)]);
+            }
+            qs += len;
         }
     }
     __syncthreads();
+    /* the last block out resets the work queue for the next launch on the stream */
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&st->item_done, 1u) == gridDim.x - 1) {
+            st->item_next = 0u;
+            st->item_done = 0u;
+        }
+    }
     if (abort_flag) {
         /* record, then let every issued copy land before the block exits */
         if (threadIdx.x == 0) {
             atomicExch(&st->err, ERR_TMA_TIMEOUT);
             const int q1 = issued_count;
             for (int q = q1 > nstage ? q1 - nstage : 0; q < q1; ++q)
-                mbar_wait(&full[stage_of(first + q)], parity_of(first + q), WAIT_LIMIT / 8);
+                mbar_wait(&full[stage_of(q)], parity_of(q), WAIT_LIMIT / 8);
         }
         __syncthreads();
         return;
     }
 
     if (SUMS != SUM_NONE) {
-        double v[NSUM];
-#pragma unroll
-        for (int s = 0; s < NSUM; ++s) v[s] = acc[s].value();
         __shared__ double tot[NSUM];
-        if (reduce_last_block<NT3>(v, partials, &st->counter, tot)) {
-            if (threadIdx.x == 0) epilogue(k, st, tot, !DF, SUMS == SUM_FULL);
+        if (last_block_ticket<NT3>(&st->counter)) {
+            sum_rows<NT3, NS>(partials, (unsigned)items, tot);
+            if (threadIdx.x < 32) epilogue(k, st, tot, !DF, SUMS == SUM_FULL, threadIdx.x);
         }
     }
 }
 
 }  // namespace
 
-bool step3_geometry_cz(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid, int &cz);
+/* SMs of the current device (148 on B200; the same figure without a device). */
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return 148;
+    }
+    if (cached[dev] == 0) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+            cudaGetLastError();
+            v = 148;
+        }
+        cached[dev] = v;
+    }
+    return cached[dev];
+}
 
 /* The tiled path covers d = 3 with n a multiple of the vector width, n >= 64
  * and n <= 1024; returns false for other shapes (the generic kernel runs).
  * Geometry: TJ rows per tile (TJ * n about 2048 sites in float, 1024 in
- * double), as many ring stages as keep two blocks per SM (4..6), and planes
- * per chunk halved from 32 (down to 8) until the grid has >= 4 waves. */
-bool step3_geometry(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid) {
-    int cz;
-    return step3_geometry_cz(k, prec, tj, nstage, smem, grid, cz);
-}
-
-bool step3_geometry_cz(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid, int &cz) {
+ * double), as many ring stages as keep two blocks per SM (4..6), one block
+ * per resident slot (2 per SM), and the number of plane parts that balances
+ * the fixed cost of every item against the part-filled last round.
+ * CB_STEP3_PARTS overrides the parts. */
+bool step3_geometry_parts(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid,
+                          int &parts) {
     if (k.d != 3) return false;
     const int n = k.n;
     const int esz = prec == P_FP64 ? 8 : 4;
@@ -316,33 +505,66 @@ bool step3_geometry_cz(const StepConst &k, int prec, int &tj, int &nstage, size_
         if (n % t == 0) tj = t;
     const bool df = k.expanding != 0;
     const size_t stage = ((size_t)(tj + 2) + (size_t)(tj + (df ? 2 : 0))) * n * esz;
-    const size_t budget = 110 * 1024;   /* two blocks per SM */
+    const size_t budget = 106 * 1024;   /* two blocks per SM, with their static shared memory */
     nstage = (int)((budget - HDR) / stage);
     if (nstage > 6) nstage = 6;
     if (nstage < 4) nstage = 4;
     smem = HDR + nstage * stage;
     if (smem > 220 * 1024) return false;
-    const int ntiles = n / tj;
-    cz = 32;
-    while (cz > 8 && (size_t)ntiles * ((n + cz - 1) / cz) < 4 * 2 * 148) cz /= 2;
-    grid = (unsigned)(ntiles * ((n + cz - 1) / cz));
+    const long long ntiles = n / tj;
+    const long long slots = 2LL * sm_count();
+    /* time in units of one plane of one tile. An item costs its planes plus a
+     * fixed part -- about one plane for a static background, 2.5 with
+     * drift-first (its halo planes are drifted too). Items that fit the slots
+     * at once take one item's time; a longer queue takes its share per slot
+     * plus about half an item of tail. */
+    const double fixed = df ? 2.5 : 1.0;
+    double best = 1e300;
+    parts = 1;
+    for (int P = 1; P <= n / 4; ++P) {
+        const double per_item = (double)n / P + fixed;
+        const long long nitems = ntiles * P;
+        const double cost = nitems <= slots ? per_item : (double)nitems / slots * per_item + 0.5 * per_item;
+        if (cost < best - 1e-9) {
+            best = cost;
+            parts = P;
+        }
+    }
+    const char *env = std::getenv("CB_STEP3_PARTS");
+    if (env && std::atoi(env) >= 1 && std::atoi(env) <= n) parts = std::atoi(env);
+    const long long items = ntiles * parts;
+    grid = (unsigned)(items < slots ? items : slots);
     return true;
+}
+
+bool step3_geometry(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid) {
+    int parts;
+    return step3_geometry_parts(k, prec, tj, nstage, smem, grid, parts);
+}
+
+/* Rows of partial sums the staged kernel writes: one per work item. */
+size_t step3_partial_rows(const StepConst &k, int prec) {
+    int tj, nstage, parts;
+    size_t smem;
+    unsigned grid;
+    if (!step3_geometry_parts(k, prec, tj, nstage, smem, grid, parts)) return 0;
+    return (size_t)(k.n / tj) * parts;
 }
 
 cudaError_t launch_step3(int prec, const StepConst &k, bool df, int sums, const void *phi_in, const void *pi_in,
                          void *phi_out, void *pi_out, void *le, void *lg, void *lp, DevState *st, double *partials,
                          cudaStream_t s) {
-    int tj, nstage, cz;
+    int tj, nstage, parts;
     size_t smem;
     unsigned grid;
-    if (!step3_geometry_cz(k, prec, tj, nstage, smem, grid, cz)) return cudaErrorInvalidValue;
+    if (!step3_geometry_parts(k, prec, tj, nstage, smem, grid, parts)) return cudaErrorInvalidValue;
 #define CB_LAUNCH3(T, DFv, SU)                                                                                     \
     do {                                                                                                           \
         auto fn = k_step3<T, DFv, SU>;                                                                             \
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);          \
         if (e != cudaSuccess) return e;                                                                            \
-        fn<<<grid, NT3, smem, s>>>(k, tj, nstage, cz, (const T *)phi_in, (const T *)pi_in, (T *)phi_out, (T *)pi_out, \
-                                   (T *)le, (T *)lg, (T *)lp, st, partials);                                       \
+        fn<<<grid, NT3, smem, s>>>(k, tj, nstage, parts, (const T *)phi_in, (const T *)pi_in, (T *)phi_out,        \
+                                   (T *)pi_out, (T *)le, (T *)lg, (T *)lp, st, partials);                          \
     } while (0)
     if (prec == P_FP64) {
         if (df && sums == SUM_FULL) CB_LAUNCH3(double, true, SUM_FULL);

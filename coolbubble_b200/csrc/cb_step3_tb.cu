@@ -143,9 +143,9 @@ __global__ void __launch_bounds__(TB_NT, 1)
         }
     } else {
         /* ---- consumers ---- */
-        const T dt = (T)k.dt;
+        const T dt = kc<T>(k.dt, k.dtf);
         const T fl = (T)st->fl, fv = (T)st->fv;
-        const T inv_dx2 = (T)k.inv_dx2;
+        const T inv_dx2 = kc<T>(k.inv_dx2, k.inv_dx2f);
         const int nvr = n / W;   /* vectors per row */
         const int nvr_shift = (nvr & (nvr - 1)) == 0 ? __ffs(nvr) - 1 : -1;
         auto acquire = [&](int p) -> bool {
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(TB_NT, 1)
             /* packed-pair constants: force = (fl inv_dx2) lap - fv V'(phi),
              * V'(f) = f (c2 + f (-c3 + f c4)) */
             const F2 FLX = f2_splat((float)(fl * inv_dx2)), NFV = f2_splat(-(float)fv), DT = f2_splat((float)dt);
-            const F2 C2 = f2_splat((float)k.c2), NC3 = f2_splat(-(float)k.c3), C4 = f2_splat((float)k.c4);
+            const F2 C2 = f2_splat(k.c2f), NC3 = f2_splat(-k.c3f), C4 = f2_splat(k.c4f);
             for (int v = threadIdx.x; v < nv; v += TB_NC) {
                 const int r = nvr_shift >= 0 ? (v >> nvr_shift) : v / nvr;
                 const int kk = (v - r * nvr) * W;

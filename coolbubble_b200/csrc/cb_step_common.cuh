@@ -48,6 +48,14 @@ struct Ar<float> {
     static __device__ __forceinline__ float quart(float x) { float p = x * x; return p * p; }
 };
 
+/* A run constant in the kernel's type: float kernels take the copy rounded on
+ * the host, which sits in the parameter bank (no conversion per use). */
+template <typename T>
+__device__ __forceinline__ T kc(double d, float f) {
+    if constexpr (std::is_same<T, float>::value) return f;
+    else return d;
+}
+
 /* Per-thread accumulator: double for FP64, Kahan-compensated float for FP32C. */
 template <typename T>
 struct Acc;
@@ -78,7 +86,7 @@ __device__ __forceinline__ T dV(const StepConst &k, T f) {
     if constexpr (std::is_same<T, double>::value) {
         return A::add(A::sub(A::mul(k.c2, f), A::mul(k.c3, A::sq(f))), A::mul(k.c4, A::cube(f)));
     } else {
-        return f * ((float)k.c2 + f * (-(float)k.c3 + f * (float)k.c4));
+        return f * (k.c2f + f * (-k.c3f + f * k.c4f));
     }
 }
 
@@ -90,23 +98,76 @@ __device__ __forceinline__ T Vpot(const StepConst &k, T f) {
                       k.dv);
     } else {
         float f2 = f * f;
-        return (float)k.dv + f2 * ((float)k.v2 + f * (-(float)k.v3 + f * (float)k.v4));
+        return k.dvf + f2 * (k.v2f + f * (-k.v3f + f * k.v4f));
     }
 }
 
-/* Block-wide reduction of NSUM doubles into partials[block]; the last block
- * to finish adds all partials in a fixed order and returns true with the
- * totals in tot[] (valid in thread 0). NT is the block size (a multiple of
- * 32); the fixed order makes the result independent of which block is last. */
+/* All threads of a block: after the block's partial rows are written, take a
+ * ticket; returns true (in every thread) in the last block to finish, which
+ * also sets the ticket counter back to zero for the next launch. */
 template <int NT>
+__device__ bool last_block_ticket(unsigned int *counter) {
+    __shared__ bool is_last;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+        is_last = (atomicAdd(counter, 1u) == nblocks - 1);
+        if (is_last) *counter = 0u;
+    }
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+/* All threads of one block: tot[s] = sum over rows r of partials[r * NSUM + s]
+ * for s < NS (tot[NS ..) = 0), in a fixed order (thread t adds rows t, t + NT,
+ * ...; then the warps by shuffle; then the warps in order), so the result does
+ * not depend on which block runs it. tot is valid in every thread on return. */
+template <int NT, int NS = NSUM>
+__device__ void sum_rows(const double *partials, unsigned rows, double *tot) {
+    constexpr int NW = NT / 32;
+    __shared__ double red2[NW][NS];
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int lane = tid & 31, w = tid >> 5;
+    double acc[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) acc[s] = 0.0;
+    for (unsigned b = tid; b < rows; b += NT) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) acc[s] = __dadd_rn(acc[s], __ldcg(partials + (size_t)b * NSUM + s));
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        double x = acc[s];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));
+        if (lane == 0) red2[w][s] = x;
+    }
+    __syncthreads();
+    if (tid < NSUM) {
+        double x = 0.0;
+        if (tid < NS)
+            for (int i = 0; i < NW; ++i) x = __dadd_rn(x, red2[i][tid]);
+        tot[tid] = x;
+    }
+    __syncthreads();
+}
+
+/* Block-wide reduction of the first NS of the NSUM sums into partials[block]
+ * (row stride NSUM); the last block to finish adds all partials in a fixed
+ * order and returns true with the totals in tot[0 .. NS) (tot[NS ..) = 0),
+ * valid in every thread. NT is the block size (a multiple of 32); the fixed
+ * order makes the result independent of which block is last. */
+template <int NT, int NS = NSUM>
 __device__ bool reduce_last_block(double (&v)[NSUM], double *partials, unsigned int *counter, double *tot) {
     constexpr int NW = NT / 32;
     __shared__ double red[NW][NSUM];
-    __shared__ bool is_last;
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
     const int lane = tid & 31, w = tid >> 5;
 #pragma unroll
-    for (int s = 0; s < NSUM; ++s) {
+    for (int s = 0; s < NS; ++s) {
         double x = v[s];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));
@@ -115,40 +176,13 @@ __device__ bool reduce_last_block(double (&v)[NSUM], double *partials, unsigned 
     __syncthreads();
     const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
     const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    if (tid < NSUM) {
+    if (tid < NS) {
         double x = 0.0;
         for (int i = 0; i < NW; ++i) x = __dadd_rn(x, red[i][tid]);
         partials[(size_t)bid * NSUM + tid] = x;
     }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) is_last = (atomicAdd(counter, 1u) == nblocks - 1);
-    __syncthreads();
-    if (!is_last) return false;
-    __threadfence();
-    /* fixed order: thread t adds blocks t, t + NT, ...; then warps by shuffle; then warps in order */
-    double acc[NSUM];
-#pragma unroll
-    for (int s = 0; s < NSUM; ++s) acc[s] = 0.0;
-    for (unsigned b = tid; b < nblocks; b += NT) {
-#pragma unroll
-        for (int s = 0; s < NSUM; ++s) acc[s] = __dadd_rn(acc[s], __ldcg(partials + (size_t)b * NSUM + s));
-    }
-#pragma unroll
-    for (int s = 0; s < NSUM; ++s) {
-        double x = acc[s];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));
-        if (lane == 0) red[w][s] = x;
-    }
-    __syncthreads();
-    if (tid < NSUM) {
-        double x = 0.0;
-        for (int i = 0; i < NW; ++i) x = __dadd_rn(x, red[i][tid]);
-        tot[tid] = x;
-    }
-    __syncthreads();
-    if (tid == 0) *counter = 0u;
+    if (!last_block_ticket<NT>(counter)) return false;
+    sum_rows<NT, NS>(partials, nblocks, tot);
     return true;
 }
 
@@ -175,13 +209,28 @@ __device__ void set_coefficients(const StepConst &k, DevState *st) {
 /* Which sums a step kernel accumulates. */
 enum SumMode { SUM_NONE = 0, SUM_FRIEDMANN = 1, SUM_FULL = 2 };
 
-/* The scalar part of oneStep, run by one thread of the last block:
- * time-centred kinetic energy (bubble.cpp:838-843), a'' and the a/a'
- * update (747-757, 860-865), H and C (873-875), pending drift (870).
+/* The six powers of one epilogue, one per lane of the calling warp (they are
+ * independent; lanes 6..31 compute a harmless pow(1, 0)). */
+__device__ __forceinline__ double lane_pow(int lane, const double (&base)[6], const double (&ex)[6]) {
+    double b = 1.0, e = 0.0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+        if (lane == i) {
+            b = base[i];
+            e = ex[i];
+        }
+    return pow(b, e);
+}
+
+/* The scalar part of oneStep, run by all 32 lanes of one warp of the last
+ * block (every lane evaluates the same scalar arithmetic; the powers are
+ * spread over the lanes; lane 0 writes): time-centred kinetic energy
+ * (bubble.cpp:838-843), a'' and the a/a' update (747-757, 860-865), H and C
+ * (873-875), pending drift (870), and the coefficients of the next step.
  * `full`: all sums were accumulated; otherwise only those the Friedmann
  * update needs (kinetic, potential, and gradient for conformal time), and
  * only the background advances. */
-__device__ void epilogue(const StepConst &k, DevState *st, const double *tot, bool static_bg, bool full) {
+__device__ void epilogue(const StepConst &k, DevState *st, const double *tot, bool static_bg, bool full, int lane) {
     const double dxLD = k.dxLD, dxLD2 = __dmul_rn(k.dxLD, k.dxLD);
     const double epot = __dmul_rn(tot[S_EP], dxLD);
     const double egrad = __dmul_rn(tot[S_EG], dxLD);
@@ -189,21 +238,6 @@ __device__ void epilogue(const StepConst &k, DevState *st, const double *tot, bo
     const double ekprev = static_bg ? __dmul_rn(tot[S_EKIN_IN], dxLD) : st->ekin_half_prev;
     const double ekin = __dmul_rn(0.5, __dadd_rn(ekhalf, ekprev));
     const double etot = __dadd_rn(__dadd_rn(ekin, epot), egrad);
-    st->ekin_half_prev = ekhalf;
-    if (full) {
-        st->epot = epot;
-        st->egrad = egrad;
-        st->ekin = ekin;
-        st->etot = etot;
-        st->avphi = __dmul_rn(tot[S_PHI], dxLD);
-        st->avphip = __dmul_rn(tot[S_V], dxLD);
-        st->ekin_var = __dmul_rn(tot[Q_EK], dxLD2);
-        st->epot_var = __dmul_rn(tot[Q_EP], dxLD2);
-        st->egrad_var = __dmul_rn(tot[Q_EG], dxLD2);
-        st->etot_var = __dmul_rn(tot[Q_ET], dxLD2);
-        st->avphi_var = __dmul_rn(tot[Q_PHI], dxLD2);
-        st->avphip_var = __dmul_rn(tot[Q_V], dxLD2);
-    }
 
     const double mpl2 = __dmul_rn(__dmul_rn(3.0, k.mpl), k.mpl);
     double a = st->a, ap = st->ap;
@@ -222,15 +256,49 @@ __device__ void epilogue(const StepConst &k, DevState *st, const double *tot, bo
     const double a_old = a;
     a = __dadd_rn(a, __dmul_rn(k.dt, ap));
     const double a_half = __dmul_rn(0.5, __dadd_rn(a, a_old));
-    st->H = __ddiv_rn(ap_atn, a_old);
+    const double H = __ddiv_rn(ap_atn, a_old);
+    const double a_kin = __dadd_rn(a, __dmul_rn(__dmul_rn(0.5, k.dt), ap));
+    const int d = k.d, al = k.alpha;
+    /* C's a^(2 alpha), the pending drift a_half^(alpha - d), and the next
+     * step's a^(d-2+alpha), a^(d+alpha), a_kin^(-2d), a_kin^(-d) */
+    const double base[6] = {a_old, a_half, a, a, a_kin, a_kin};
+    const double ex[6] = {(double)(2 * al), (double)(-d + al), (double)(d - 2 + al), (double)(d + al),
+                          (double)(-2 * d), (double)(-d)};
+    const double mine = lane_pow(lane, base, ex);
+    double pw[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) pw[i] = __shfl_sync(0xffffffffu, mine, i);
+    __syncwarp();
+    if (lane != 0) return;
+    st->ekin_half_prev = ekhalf;
+    if (full) {
+        st->epot = epot;
+        st->egrad = egrad;
+        st->ekin = ekin;
+        st->etot = etot;
+        st->avphi = __dmul_rn(tot[S_PHI], dxLD);
+        st->avphip = __dmul_rn(tot[S_V], dxLD);
+        st->ekin_var = __dmul_rn(tot[Q_EK], dxLD2);
+        st->epot_var = __dmul_rn(tot[Q_EP], dxLD2);
+        st->egrad_var = __dmul_rn(tot[Q_EG], dxLD2);
+        st->etot_var = __dmul_rn(tot[Q_ET], dxLD2);
+        st->avphi_var = __dmul_rn(tot[Q_PHI], dxLD2);
+        st->avphip_var = __dmul_rn(tot[Q_V], dxLD2);
+    }
+    st->H = H;
     if (full)   /* C needs the full Etot; only reported at steps that measure all sums */
-        st->C = k.expanding ? __dsub_rn(__dmul_rn(st->H, st->H),
-                                        __ddiv_rn(__dmul_rn(pow(a_old, (double)(2 * k.alpha)), etot), mpl2))
-                            : 0.0;
+        st->C = k.expanding ? __dsub_rn(__dmul_rn(H, H), __ddiv_rn(__dmul_rn(pw[0], etot), mpl2)) : 0.0;
     st->a = a;
     st->ap = ap;
-    st->drift_p = pow(a_half, (double)(-k.d + k.alpha));
-    set_coefficients(k, st);
+    st->drift_p = pw[1];
+    st->fl = pw[2];
+    st->fv = pw[3];
+    st->a_kin = a_kin;
+    st->kin_w = __dmul_rn(0.5, pw[4]);
+    st->vel_w = pw[5];
+    st->adx = __dmul_rn(a, k.dx);
+    st->inv_adx = __ddiv_rn(1.0, st->adx);
+    st->adx_pow2 = is_pow2(st->adx);
 }
 
 }  // namespace

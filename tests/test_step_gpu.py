@@ -220,7 +220,12 @@ def test_tiled_kernel_equals_generic_kernel_fp64(case, monkeypatch):
     a = tiled.step(25, sums=True, local=True)
     b = generic.step(25, sums=True, local=True)
     for key in a:
-        assert a[key] == pytest.approx(b[key], rel=1e-14, abs=1e-300), key
+        # C = H^2 - a^(2 alpha) Etot / (3 Mpl^2) cancels: judged on the H^2 scale;
+        # signed sums (<phi>, <phidot>) on the scale of sqrt(N sum x^2), a bound on sum |x|
+        scale = abs(b["H"]) ** 2 if key == "C" else abs(b[key])
+        if key in ("avphi", "avphip"):
+            scale = max(scale, (n ** d * b[key + "_var"]) ** 0.5)
+        assert abs(a[key] - b[key]) <= 1e-14 * scale + 1e-300, key
     fa, fb = tiled.fields(), generic.fields()
     for key in fa:
         np.testing.assert_array_equal(fa[key], fb[key])
