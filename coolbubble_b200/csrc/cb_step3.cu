@@ -63,6 +63,19 @@ __device__ __forceinline__ bool consumer_any(bool x) {
     return r != 0;
 }
 
+/* Ring cursor: the stage of a ring position and the phase parity of its
+ * mbarriers, advanced one position at a time (no division per plane). */
+struct Cursor {
+    int s;
+    uint32_t ph;
+    __device__ __forceinline__ void next(int nstage) {
+        if (++s == nstage) {
+            s = 0;
+            ph ^= 1u;
+        }
+    }
+};
+
 /* Shared-memory layout of one stage: phi rows [TJ + 2][n] (row 0 and TJ + 1
  * are the halo rows), then pi rows [TJ + 2*DF][n] (drift-first also needs the
  * halo rows of pi to drift the halo of phi). */
@@ -113,8 +126,6 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
     const size_t plane = (size_t)n * n;
     const uint32_t tx_bytes = (uint32_t)(((size_t)(tj + 2) + g.pi_rows()) * row_bytes);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    auto stage_of = [&](int q) { return q % nstage; };
-    auto parity_of = [&](int q) { return (uint32_t)((q / nstage) & 1); };
     auto item_of = [&](int it, int &t, int &p0, int &p1) {
         const int c = it / ntiles;
         t = it % ntiles;
@@ -140,9 +151,8 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         /* ---- producer warp: lane 0 takes items from the queue and issues the
          *      bulk copies of their planes, reusing a stage once all consumer
          *      warps released the plane it held ---- */
-        auto issue = [&](int q, int pl, int j0) {
-            const int s = q % nstage;
-            const int pw = (pl + n) % n;
+        auto issue = [&](int s, int pl, int j0) {
+            const int pw = pl < 0 ? pl + n : (pl >= n ? pl - n : pl);
             const int jm = (j0 - 1 + n) % n, jp = (j0 + tj) % n;
             T *dst = ring + (size_t)s * stage_elems;
             const T *src_phi = phi_in + (size_t)pw * plane;
@@ -161,10 +171,12 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                 bulk_g2s(dpi, src_pi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
             }
         };
-        /* stage reuse: position q goes where position q - nstage was, once released */
-        auto free_for = [&](int q) -> bool {
-            const int use = q / nstage;
-            return use == 0 || mbar_wait(&empty[q % nstage], (uint32_t)((use - 1) & 1), WAIT_LIMIT);
+        /* stage reuse: position q goes where position q - nstage was, once
+         * released; pc is the cursor of q, and q >= nstage once pc wrapped */
+        Cursor pc{0, 0u};
+        bool wrapped = false;
+        auto free_for = [&]() -> bool {
+            return !wrapped || mbar_wait(&empty[pc.s], pc.ph ^ 1u, WAIT_LIMIT);
         };
         if (lane == 0) {
             int q = 0;
@@ -181,7 +193,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                 int t, p0, p1;
                 item_of(cur, t, p0, p1);
                 for (int pl = p0 - 1; pl <= p1; ++pl, ++q) {
-                    if (!free_for(q)) {
+                    if (!free_for()) {
                         atomicExch(&abort_flag, 1);
                         ok = false;
                         break;
@@ -190,7 +202,9 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                         ok = false;
                         break;
                     }
-                    issue(q, pl, t * tj);
+                    issue(pc.s, pl, t * tj);
+                    pc.next(nstage);
+                    if (pc.s == 0) wrapped = true;
                 }
                 /* the next item is taken only now, with this one fully issued:
                  * taken earlier, a block would hold back an item an idle block
@@ -214,35 +228,39 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         const int nvec_row = n / W;
         const int nvec = tj * nvec_row;
         const int row_step = NC / nvec_row, vec_step = NC % nvec_row;
-        const bool want_eg = SUMS == SUM_FULL || k.alpha == 1;
-        /* wait for ring position q to land */
-        auto acquire = [&](int q) -> bool {
-            const bool ok = abort_flag == 0 && mbar_wait(&full[stage_of(q)], parity_of(q), WAIT_LIMIT);
+        constexpr bool want_eg = SUMS == SUM_FULL || SUMS == SUM_FRIEDMANN_EG;
+        /* wait for the ring position under cursor c to land */
+        auto acquire = [&](const Cursor &c) -> bool {
+            const bool ok = abort_flag == 0 && mbar_wait(&full[c.s], c.ph, WAIT_LIMIT);
             if (!ok) atomicExch(&abort_flag, 1);
             return ok;
         };
+        const int stage_n = (int)stage_elems;          /* elements per stage (< 2^31) */
+        const int pi_off = (int)g.phi_elems();
         /* drift-first: the pending drift phi += (dt pi) p of the previous step
          * (bubble.cpp:867-870) is applied once to each plane as it lands, in
          * place, to all its rows (halo rows included: the pi stage rows line up
          * with the phi rows); every later read then sees the drifted field */
-        auto drift_plane = [&](int q) {
-            T *S = ring + (size_t)stage_of(q) * stage_elems;
-            const T *Pi = S + g.phi_elems();
-            const int nv = (tj + 2) * n / W;
-            for (int v = threadIdx.x; v < nv; v += NC) {
-                VT f = *reinterpret_cast<const VT *>(S + (size_t)v * W);
-                const VT mom = *reinterpret_cast<const VT *>(Pi + (size_t)v * W);
+        const int nv_drift = (tj + 2) * n / W;
+        auto drift_plane = [&](const Cursor &c) {
+            T *S = ring + c.s * stage_n;
+            const T *Pi = S + pi_off;
+            for (int v = threadIdx.x; v < nv_drift; v += NC) {
+                VT f = *reinterpret_cast<const VT *>(S + v * W);
+                const VT mom = *reinterpret_cast<const VT *>(Pi + v * W);
 #pragma unroll
                 for (int t = 0; t < W; ++t)
                     Vec<T>::set(f, t, A::add(Vec<T>::get(f, t), A::mul(A::mul(dt, Vec<T>::get(mom, t)), p)));
-                *reinterpret_cast<VT *>(S + (size_t)v * W) = f;
+                *reinterpret_cast<VT *>(S + v * W) = f;
             }
         };
+        /* this thread's first (row, vector) in a tile plane; later ones step by NC */
+        const int r_first = threadIdx.x / nvec_row, kv_first = threadIdx.x % nvec_row;
         /* drift-first and the sums run consumer barriers (per plane, per item):
          * every consumer warp then takes the same exit (a vote in the barrier)
          * when a wait runs out */
         bool run = true;
-        int qs = 0;   /* ring position of the item's first plane */
+        Cursor cq{0, 0u};   /* ring cursor of the item's first plane */
         for (int j = 0; run; ++j) {
             if (abort_flag != 0 || !mbar_wait(&item_full[j % IQ], (uint32_t)((j / IQ) & 1), WAIT_LIMIT)) {
                 atomicExch(&abort_flag, 1);
@@ -261,54 +279,58 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
             int t, p0, p1;
             item_of(it, t, p0, p1);
             const int j0 = t * tj;
-            const int len = p1 - p0 + 2;
             if (SUMS != SUM_NONE) {
 #pragma unroll
                 for (int s = 0; s < NSUM; ++s) acc[s] = Acc<T>{};
             }
-            bool ok = acquire(qs) && acquire(qs + 1);
+            /* cm, c0, cp: cursors of planes i - 1, i, i + 1 */
+            Cursor cm = cq, c0 = cq;
+            c0.next(nstage);
+            bool ok = acquire(cm) && acquire(c0);
             if (UNI) {
                 if (DF && ok) {
-                    drift_plane(qs);
-                    drift_plane(qs + 1);
+                    drift_plane(cm);
+                    drift_plane(c0);
                 }
                 if (consumer_any(!ok)) { run = false; break; }
             } else if (!ok) {
                 run = false;
                 break;
             }
+            Cursor cp = c0;
+            cp.next(nstage);
             for (int i = p0; i < p1; ++i) {
-                const int qi = qs + (i - p0) + 1;   /* position of plane i */
-                ok = acquire(qi + 1);
+                ok = acquire(cp);
                 if (UNI) {
-                    if (DF && ok) drift_plane(qi + 1);
+                    if (DF && ok) drift_plane(cp);
                     if (consumer_any(!ok)) { run = false; break; }
                 } else if (!ok) {
                     run = false;
                     break;
                 }
-                const T *Sm = ring + (size_t)stage_of(qi - 1) * stage_elems;
-                const T *S0 = ring + (size_t)stage_of(qi) * stage_elems;
-                const T *Sp = ring + (size_t)stage_of(qi + 1) * stage_elems;
-                const T *P0 = S0 + g.phi_elems() + (DF ? n : 0);
+                const T *Sm = ring + cm.s * stage_n;
+                const T *S0 = ring + c0.s * stage_n;
+                const T *Sp = ring + cp.s * stage_n;
+                const T *P0 = S0 + pi_off + (DF ? n : 0);
                 const size_t gbase = ((size_t)i * n + j0) * n;
-                /* (row, vector) of v, stepped by NC without a division per vector */
-                int r = threadIdx.x / nvec_row, kv = threadIdx.x % nvec_row;
+                T *const phi_o = phi_out + gbase;
+                T *const pi_o = pi_out + gbase;
+                int r = r_first, kv = kv_first;
                 for (int v = threadIdx.x; v < nvec; v += NC, r += row_step, kv += vec_step) {
                     if (kv >= nvec_row) {
                         kv -= nvec_row;
                         ++r;
                     }
                     const int kk = kv * W;
-                    const size_t c_off = (size_t)(r + 1) * n + kk;
+                    const int c_off = (r + 1) * n + kk;
                     const VT c = *reinterpret_cast<const VT *>(S0 + c_off);
                     const VT um = *reinterpret_cast<const VT *>(S0 + c_off - n);
                     const VT up = *reinterpret_cast<const VT *>(S0 + c_off + n);
                     const VT im = *reinterpret_cast<const VT *>(Sm + c_off);
                     const VT ip = *reinterpret_cast<const VT *>(Sp + c_off);
-                    const VT pv = *reinterpret_cast<const VT *>(P0 + (size_t)r * n + kk);
-                    const size_t lo = (size_t)(r + 1) * n + (kk == 0 ? n - 1 : kk - 1);
-                    const size_t ro = (size_t)(r + 1) * n + (kk + W == n ? 0 : kk + W);
+                    const VT pv = *reinterpret_cast<const VT *>(P0 + r * n + kk);
+                    const int lo = (r + 1) * n + (kk == 0 ? n - 1 : kk - 1);
+                    const int ro = (r + 1) * n + (kk + W == n ? 0 : kk + W);
                     const T left = S0[lo];
                     const T right = S0[ro];
                     VT phi_new, pi_new, vek, veg, vep;
@@ -343,7 +365,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                         Vec<T>::set(phi_new, s, DF ? cur : A::add(cur, A::mul(dt, pn)));
                         if (SUMS != SUM_NONE) {
                             T eg = (T)0;
-                            if (want_eg) {
+                            if constexpr (want_eg) {
                                 /* forward gradients: x <- axis 1, y <- axis 0, z <- axis 2 (bubble.cpp:794-801) */
                                 const T gx = grad(A::sub(Vec<T>::get(up, s), cur));
                                 const T gy = grad(A::sub(nxt, cur));
@@ -354,7 +376,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                             const T ek = A::mul(A::mul(kin_w, pn), pn);
                             put(S_EK, ek);
                             put(S_EP, ep);
-                            if (want_eg) put(S_EG, eg);
+                            if constexpr (want_eg) put(S_EG, eg);
                             if (SUMS == SUM_FULL) {
                                 const T vv = A::mul(pn, vel_w);
                                 const T et = A::add(A::add(ek, eg), ep);
@@ -377,7 +399,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                         if (SUMS != SUM_NONE) {
                             acc[S_EK].add(part[S_EK]);
                             acc[S_EP].add(part[S_EP]);
-                            if (want_eg) acc[S_EG].add(part[S_EG]);
+                            if constexpr (want_eg) acc[S_EG].add(part[S_EG]);
                         }
                         if (SUMS == SUM_FULL) {
 #pragma unroll
@@ -385,13 +407,13 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                                 if (s != S_EK && s != S_EP && s != S_EG) acc[s].add(part[s]);
                         }
                     }
-                    const size_t o = gbase + (size_t)r * n + kk;
-                    *reinterpret_cast<VT *>(pi_out + o) = pi_new;
-                    *reinterpret_cast<VT *>(phi_out + o) = phi_new;
+                    const int o = r * n + kk;
+                    *reinterpret_cast<VT *>(pi_o + o) = pi_new;
+                    *reinterpret_cast<VT *>(phi_o + o) = phi_new;
                     if (SUMS == SUM_FULL && k.want_local) {
-                        *reinterpret_cast<VT *>(loc_ek + o) = vek;
-                        *reinterpret_cast<VT *>(loc_eg + o) = veg;
-                        *reinterpret_cast<VT *>(loc_ep + o) = vep;
+                        *reinterpret_cast<VT *>(loc_ek + gbase + o) = vek;
+                        *reinterpret_cast<VT *>(loc_eg + gbase + o) = veg;
+                        *reinterpret_cast<VT *>(loc_ep + gbase + o) = vep;
                     }
                 }
                 /* this warp no longer needs plane i - 1; with drift-first the plane was
@@ -399,7 +421,10 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                  * the copy that will refill the stage */
                 if (DF) fence_proxy_async();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&empty[stage_of(qi - 1)]);
+                if (lane == 0) mbar_arrive(&empty[cm.s]);
+                cm = c0;
+                c0 = cp;
+                cp.next(nstage);
             }
             if (!run) break;
             if (SUMS != SUM_NONE) {
@@ -424,14 +449,15 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                     partials[(size_t)it * NSUM + lane] = x;
                 }
             }
-            /* the item's last two planes */
+            /* the item's last two planes (p1 - 1 and p1, under cm and c0); the
+             * next item starts at the position after them */
             if (DF) fence_proxy_async();
             __syncwarp();
             if (lane == 0) {
-                mbar_arrive(&empty[stage_of(qs + len - 2)]);
-                mbar_arrive(&empty[stage_of(qs + len - 1)]);
+                mbar_arrive(&empty[cm.s]);
+                mbar_arrive(&empty[c0.s]);
             }
-            qs += len;
+            cq = cp;
         }
     }
     __syncthreads();
@@ -449,7 +475,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
             atomicExch(&st->err, ERR_TMA_TIMEOUT);
             const int q1 = issued_count;
             for (int q = q1 > nstage ? q1 - nstage : 0; q < q1; ++q)
-                mbar_wait(&full[stage_of(q)], parity_of(q), WAIT_LIMIT / 8);
+                mbar_wait(&full[q % nstage], (uint32_t)((q / nstage) & 1), WAIT_LIMIT / 8);
         }
         __syncthreads();
         return;
@@ -568,11 +594,13 @@ cudaError_t launch_step3(int prec, const StepConst &k, bool df, int sums, const 
     } while (0)
     if (prec == P_FP64) {
         if (df && sums == SUM_FULL) CB_LAUNCH3(double, true, SUM_FULL);
+        else if (df && k.alpha == 1) CB_LAUNCH3(double, true, SUM_FRIEDMANN_EG);
         else if (df) CB_LAUNCH3(double, true, SUM_FRIEDMANN);
         else if (sums == SUM_FULL) CB_LAUNCH3(double, false, SUM_FULL);
         else CB_LAUNCH3(double, false, SUM_NONE);
     } else {
         if (df && sums == SUM_FULL) CB_LAUNCH3(float, true, SUM_FULL);
+        else if (df && k.alpha == 1) CB_LAUNCH3(float, true, SUM_FRIEDMANN_EG);
         else if (df) CB_LAUNCH3(float, true, SUM_FRIEDMANN);
         else if (sums == SUM_FULL) CB_LAUNCH3(float, false, SUM_FULL);
         else CB_LAUNCH3(float, false, SUM_NONE);

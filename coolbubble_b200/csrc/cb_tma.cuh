@@ -35,10 +35,27 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-/* Bounded wait: false after ~limit cycles. */
+/* try_wait with a suspend-time hint: a waiting thread may sleep up to
+ * hint_ns in the hardware (woken when the phase completes) instead of
+ * spinning, so waiting warps take no issue slots from working ones. */
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
+/* Bounded wait: false after ~limit cycles. The first test is a plain one
+ * (the phase is usually complete already); retries sleep in the hardware. */
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
+    if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity)) {
+    while (!mbar_try_wait_sleep(bar, parity, 100000u)) {
         if (clock64() - t0 > limit) return false;
     }
     return true;
