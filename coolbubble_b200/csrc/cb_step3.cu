@@ -229,6 +229,12 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         const int nvec = tj * nvec_row;
         const int row_step = NC / nvec_row, vec_step = NC % nvec_row;
         constexpr bool want_eg = SUMS == SUM_FULL || SUMS == SUM_FRIEDMANN_EG;
+        constexpr bool PACKED = std::is_same<T, float>::value && (SUMS == SUM_NONE || SUMS == SUM_FRIEDMANN);
+        /* packed-pair constants of the f32x2 path (unused otherwise) */
+        const F2 P_FL = f2_splat((float)fl), P_IDX2 = f2_splat((float)inv_dx2), P_NFV = f2_splat(-(float)fv);
+        const F2 P_DT = f2_splat((float)dt), P_KW = f2_splat((float)kin_w);
+        const F2 P_C2 = f2_splat(k.c2f), P_NC3 = f2_splat(-k.c3f), P_C4 = f2_splat(k.c4f);
+        const F2 P_V2 = f2_splat(k.v2f), P_NV3 = f2_splat(-k.v3f), P_V4 = f2_splat(k.v4f), P_DV = f2_splat(k.dvf);
         /* wait for the ring position under cursor c to land */
         auto acquire = [&](const Cursor &c) -> bool {
             const bool ok = abort_flag == 0 && mbar_wait(&full[c.s], c.ph, WAIT_LIMIT);
@@ -334,6 +340,43 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                     const T left = S0[lo];
                     const T right = S0[ro];
                     VT phi_new, pi_new, vek, veg, vep;
+                    if constexpr (PACKED) {
+                    /* float, no sums or the Friedmann sums only: the four sites as two
+                     * packed pairs (f32x2 arithmetic, one instruction per pair), the
+                     * same operations in the same order as the scalar path */
+                    const F2 c01 = f2_pack(c.x, c.y), c23 = f2_pack(c.z, c.w);
+                    const F2 km01 = f2_pack(left, c.x), mid = f2_pack(c.y, c.z), kp23 = f2_pack(c.w, right);
+                    F2 phi01, pi01, phi23, pi23, ek01, ek23, ep01, ep23;
+                    auto pair = [&](F2 cc, F2 umm, F2 upp, F2 imm, F2 ipp, F2 kmm, F2 kpp, F2 pp, F2 &phi_n,
+                                    F2 &pi_n, F2 &ek, F2 &ep) {
+                        const F2 two = f2_add(cc, cc);
+                        const F2 t0 = f2_add(f2_sub(ipp, two), imm);
+                        const F2 t1 = f2_add(f2_sub(upp, two), umm);
+                        const F2 t2 = f2_add(f2_sub(kpp, two), kmm);
+                        const F2 lap = f2_add(f2_add(t0, t1), t2);
+                        /* V'(f) = f (c2 + f (-c3 + f c4)) */
+                        const F2 h = f2_fma(cc, f2_fma(cc, P_C4, P_NC3), P_C2);
+                        const F2 force = f2_fma(f2_mul(P_FL, lap), P_IDX2, f2_mul(P_NFV, f2_mul(cc, h)));
+                        pi_n = f2_fma(P_DT, force, pp);
+                        phi_n = DF ? cc : f2_fma(P_DT, pi_n, cc);
+                        if constexpr (SUMS == SUM_FRIEDMANN) {
+                            ek = f2_mul(f2_mul(P_KW, pi_n), pi_n);
+                            /* V(f) = DeltaV + f^2 (v2 + f (-v3 + f v4)) */
+                            ep = f2_fma(f2_mul(cc, cc), f2_fma(cc, f2_fma(cc, P_V4, P_NV3), P_V2), P_DV);
+                        }
+                    };
+                    pair(c01, f2_pack(um.x, um.y), f2_pack(up.x, up.y), f2_pack(im.x, im.y), f2_pack(ip.x, ip.y),
+                         km01, mid, f2_pack(pv.x, pv.y), phi01, pi01, ek01, ep01);
+                    pair(c23, f2_pack(um.z, um.w), f2_pack(up.z, up.w), f2_pack(im.z, im.w), f2_pack(ip.z, ip.w),
+                         mid, kp23, f2_pack(pv.z, pv.w), phi23, pi23, ek23, ep23);
+                    phi_new = make_float4(f2_lo(phi01), f2_hi(phi01), f2_lo(phi23), f2_hi(phi23));
+                    pi_new = make_float4(f2_lo(pi01), f2_hi(pi01), f2_lo(pi23), f2_hi(pi23));
+                    if constexpr (SUMS == SUM_FRIEDMANN) {
+                        const F2 ek = f2_add(ek01, ek23), ep = f2_add(ep01, ep23);
+                        acc[S_EK].add(f2_lo(ek) + f2_hi(ek));
+                        acc[S_EP].add(f2_lo(ep) + f2_hi(ep));
+                    }
+                    } else {
                     /* float: the sites of a vector are summed plainly (W terms), then
                      * the vector's sum enters the compensated per-thread accumulator;
                      * double: every site enters the accumulator in site order */
@@ -406,6 +449,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                             for (int s = 0; s < NSUM; ++s)
                                 if (s != S_EK && s != S_EP && s != S_EG) acc[s].add(part[s]);
                         }
+                    }
                     }
                     const int o = r * n + kk;
                     *reinterpret_cast<VT *>(pi_o + o) = pi_new;
