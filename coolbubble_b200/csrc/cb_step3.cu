@@ -43,13 +43,11 @@ namespace {
 constexpr int CW = 8;                 /* consumer warps */
 constexpr int NC = CW * 32;           /* consumer threads */
 constexpr int NT3 = NC + 32;          /* plus one producer warp */
-constexpr int HDR = 256;              /* full[8], empty[8] and item_full[IQ] mbarriers */
+constexpr int HDR = 256;              /* full[8], empty[8], item_full[IQ] and drifted[8] mbarriers */
 constexpr int IQ = 8;                 /* items the producer may hand over ahead of the consumers */
 
-/* barrier among the consumer warps only (id 1; id 0 is __syncthreads) */
-__device__ __forceinline__ void consumer_bar() { asm volatile("bar.sync 1, %0;" ::"n"(NC) : "memory"); }
-
-/* the same barrier, also returning whether any consumer thread passed true */
+/* barrier among the consumer warps only (id 1; id 0 is __syncthreads),
+ * returning whether any consumer thread passed true */
 __device__ __forceinline__ bool consumer_any(bool x) {
     uint32_t r;
     asm volatile(
@@ -105,6 +103,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
     uint64_t *full = reinterpret_cast<uint64_t *>(smraw);
     uint64_t *empty = full + 8;
     uint64_t *item_full = full + 16;
+    uint64_t *drifted = full + 24;
     T *ring = reinterpret_cast<T *>(smraw + HDR);
     __shared__ int abort_flag;
     __shared__ int issued_count;
@@ -139,6 +138,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         for (int s = 0; s < nstage; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], CW);
+            mbar_init(&drifted[s], NC);
         }
         for (int s = 0; s < IQ; ++s) mbar_init(&item_full[s], 1);
         fence_mbar_init();
@@ -246,9 +246,12 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         /* drift-first: the pending drift phi += (dt pi) p of the previous step
          * (bubble.cpp:867-870) is applied once to each plane as it lands, in
          * place, to all its rows (halo rows included: the pi stage rows line up
-         * with the phi rows); every later read then sees the drifted field */
+         * with the phi rows); every later read then sees the drifted field.
+         * Each thread drifts its share of a plane two planes ahead of the one it
+         * computes and arrives on the plane's drift mbarrier, so the consumer
+         * warps only wait for each other where a plane is first read. */
         const int nv_drift = (tj + 2) * n / W;
-        auto drift_plane = [&](const Cursor &c) {
+        auto drift_share = [&](const Cursor &c) {
             T *S = ring + c.s * stage_n;
             const T *Pi = S + pi_off;
             for (int v = threadIdx.x; v < nv_drift; v += NC) {
@@ -259,12 +262,20 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                     Vec<T>::set(f, t, A::add(Vec<T>::get(f, t), A::mul(A::mul(dt, Vec<T>::get(mom, t)), p)));
                 *reinterpret_cast<VT *>(S + v * W) = f;
             }
+            /* every consumer thread arrives once its own share is written */
+            mbar_arrive(&drifted[c.s]);
+        };
+        /* wait until every consumer thread drifted its share of the plane under c */
+        auto drifted_wait = [&](const Cursor &c) -> bool {
+            const bool ok = abort_flag == 0 && mbar_wait(&drifted[c.s], c.ph, WAIT_LIMIT);
+            if (!ok) atomicExch(&abort_flag, 1);
+            return ok;
         };
         /* this thread's first (row, vector) in a tile plane; later ones step by NC */
         const int r_first = threadIdx.x / nvec_row, kv_first = threadIdx.x % nvec_row;
-        /* drift-first and the sums run consumer barriers (per plane, per item):
-         * every consumer warp then takes the same exit (a vote in the barrier)
-         * when a wait runs out */
+        /* drift-first and the sums run consumer barriers (two per item): every
+         * consumer warp then takes the same exit (a vote in the barrier) when a
+         * wait runs out */
         bool run = true;
         Cursor cq{0, 0u};   /* ring cursor of the item's first plane */
         for (int j = 0; run; ++j) {
@@ -292,26 +303,27 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
             /* cm, c0, cp: cursors of planes i - 1, i, i + 1 */
             Cursor cm = cq, c0 = cq;
             c0.next(nstage);
-            bool ok = acquire(cm) && acquire(c0);
-            if (UNI) {
-                if (DF && ok) {
-                    drift_plane(cm);
-                    drift_plane(c0);
-                }
-                if (consumer_any(!ok)) { run = false; break; }
-            } else if (!ok) {
-                run = false;
-                break;
-            }
             Cursor cp = c0;
             cp.next(nstage);
-            for (int i = p0; i < p1; ++i) {
-                ok = acquire(cp);
-                if (UNI) {
-                    if (DF && ok) drift_plane(cp);
-                    if (consumer_any(!ok)) { run = false; break; }
-                } else if (!ok) {
-                    run = false;
+            /* a wait of this thread ran out: it stops work and leaves with the
+             * others at the item's closing vote (UNI) or at once (otherwise) */
+            bool bad;
+            if (DF) {
+                /* the item's first three planes are drifted up front; later
+                 * planes two ahead of the one computed */
+                bad = !(acquire(cm) && acquire(c0) && acquire(cp));
+                if (!bad) {
+                    drift_share(cm);
+                    drift_share(c0);
+                    drift_share(cp);
+                    bad = !(drifted_wait(cm) && drifted_wait(c0));
+                }
+            } else {
+                bad = !(acquire(cm) && acquire(c0));
+            }
+            for (int i = p0; !bad && i < p1; ++i) {
+                if (DF ? !drifted_wait(cp) : !acquire(cp)) {
+                    bad = true;
                     break;
                 }
                 const T *Sm = ring + cm.s * stage_n;
@@ -469,8 +481,19 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                 cm = c0;
                 c0 = cp;
                 cp.next(nstage);
+                if (DF && i + 2 <= p1) {
+                    /* plane i + 2 (now under cp): this thread's share of its drift */
+                    if (!acquire(cp)) {
+                        bad = true;
+                        break;
+                    }
+                    drift_share(cp);
+                }
             }
-            if (!run) break;
+            if (!UNI && bad) {
+                run = false;
+                break;
+            }
             if (SUMS != SUM_NONE) {
                 /* the item's sums: per warp by shuffle, then warp 0 adds the warps
                  * in order into the item's own row of partials (fixed place, fixed
@@ -485,7 +508,13 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                     for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));
                     if (lane == 0) item_red[j & 1][warp][s] = x;
                 }
-                consumer_bar();
+            }
+            /* closing vote of the item (also the barrier of its sums) */
+            if (UNI && consumer_any(bad)) {
+                run = false;
+                break;
+            }
+            if (SUMS != SUM_NONE) {
                 if (warp == 0 && lane < NS) {
                     double x = 0.0;
 #pragma unroll
