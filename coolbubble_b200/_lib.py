@@ -77,6 +77,7 @@ _SIGS = {
     "cb_device_error": (C.c_int, [_h, C.POINTER(C.c_int)]),
     "cb_get_fields": (C.c_int, [_h, _dp, _dp, _dp, _dp, _dp]),
     "cb_get_fields_f32": (C.c_int, [_h, _fp, _fp, _fp, _fp, _fp]),
+    "cb_get_line": (C.c_int, [_h, C.c_int, C.c_int, C.c_int, C.c_int, _dp]),
     "cb_nbins": (C.c_int, [C.c_int, C.c_int]),
     "cb_power_spectrum": (C.c_int, [_h, _dp, _dp, _dp, C.c_int]),
     "cb_dft_r2c": (C.c_int, [C.c_int, C.c_int, _dp, _dp]),

@@ -123,6 +123,14 @@ class Bubble:
         check(L.lib.cb_get_fields_f32(self._h, *[L.fptr(x) for x in out]), self._h)
         return dict(zip(("phi", "pi", "ekin", "egrad", "epot"), out))
 
+    def line(self, i0, i1=0, i2=0, count=None):
+        """phi[(i0 + m) mod n, i1, i2] for m < count (default n): one line along
+        axis 0, as the wall finder reads it (bubble.cpp:588-592)."""
+        count = self.n if count is None else int(count)
+        out = np.empty(count)
+        check(L.lib.cb_get_line(self._h, int(i0), int(i1), int(i2), count, L.dptr(out)), self._h)
+        return out
+
     @property
     def phi(self):
         return self.fields(local=False)["phi"]

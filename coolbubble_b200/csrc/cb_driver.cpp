@@ -5,7 +5,8 @@
  * main.cpp:68-139, folder name 243-249, stability check 171-183, snapshot
  * schedule 201-223, loop 274-288) and the writers of src/bubble.cpp
  * (parameters.dat 1018-1032, EnergyDensities.dat 958-989, spectrum files
- * 642-709, FullField.dat 993-1006). The compile-time def.h values become
+ * 642-709, FullField.dat 993-1006) and the wall tracking of bubble.cpp:535-634
+ * (gamma.dat 1009-1015). The compile-time def.h values become
  * options (--dt, --nbubbles, ...) with def.h's defaults. Snapshots are
  * written as a text manifest plus raw float32 payloads per dataset
  * (<file>, <file>.<name>.f32), the layout of the HDF5 stand-in of this
@@ -34,7 +35,7 @@ struct Options {
     std::string out = "./";
     /* def.h values (def.h:33-76) */
     double dt = 0.004, trad = 0.2, deltar = 0.0, mpl = 200.0;
-    int nbubbles = 5, test = 0, expansion = 0, alpha = 0, memorysave = 0;
+    int nbubbles = 5, test = 0, expansion = 0, alpha = 0, memorysave = 0, walltracking = 0;
     int precision = CB_FP64;
     unsigned position_seed = 42;
     unsigned long long thermal_seed = 12345;
@@ -42,6 +43,7 @@ struct Options {
 
 const int kOutEnergyEvery = 40;    /* def.h:65 */
 const int kFull1DFieldEvery = 100; /* def.h:71 */
+const int kWallTrackEvery = 400;   /* def.h:73 */
 
 void usage(const char *prog) {
     std::cout << "Usage: " << prog << " [options]\n\n"
@@ -49,6 +51,7 @@ void usage(const char *prog) {
               << "  --snapshots <n>  --out <dir>  --no-plots  --python-dir <d>   (as the reference)\n"
               << "  --dt <value> (TIME_STEP, 0.004)  --nbubbles <n> (5)  --trad <T> (0.2)  --deltar <x> (0)\n"
               << "  --test <0|1>  --expansion <0|1>  --alpha <0|1>  --mpl <value> (200)  --memorysave <0|1>\n"
+              << "  --wall-tracking <0|1> (WallTracking, 0)\n"
               << "  --precision <fp64|fp32c>  --position-seed <n> (42)  --thermal-seed <n> (12345)\n";
 }
 
@@ -84,6 +87,7 @@ bool parse(int argc, char **argv, Options &o) {
             else if (a == "--alpha") o.alpha = std::stoi(v);
             else if (a == "--mpl") o.mpl = std::stod(v);
             else if (a == "--memorysave") o.memorysave = std::stoi(v);
+            else if (a == "--wall-tracking") o.walltracking = std::stoi(v);
             else if (a == "--position-seed") o.position_seed = (unsigned)std::stoul(v);
             else if (a == "--thermal-seed") o.thermal_seed = std::stoull(v);
             else if (a == "--precision") {
@@ -124,6 +128,13 @@ std::string four(int n) {
     return b;
 }
 
+/* Wall of the tracked bubble (bubble.hpp:89-90; bubble.cpp:164-168, 309-313). */
+struct Wall {
+    double dini = 0, width = 0, rmin = 0, rmax = 0;
+    double rn = 0, lw = 0, phi_zero = 0, phi_max = 0, mT = 0;
+    int centre[3] = {0, 0, 0};
+};
+
 struct Run {
     Options o;
     std::string folder;
@@ -131,13 +142,14 @@ struct Run {
     cb_sums line{};
     double DeltaV = 1.0;
     size_t N = 0;
+    Wall wall;
     bool fail(int st, const char *what) {
         std::cerr << "Error: " << what << ": " << cb_last_error(h) << " (" << cb_status_string(st) << ")\n";
         return false;
     }
 };
 
-/* bubble.cpp:958-965 */
+/* bubble.cpp:958-973 */
 void init_energy_file(const Run &r) {
     FILE *fp = std::fopen((r.folder + "/EnergyDensities.dat").c_str(), "w");
     if (!fp) throw std::runtime_error("Could not open EnergyDensities.dat for writing");
@@ -145,6 +157,13 @@ void init_energy_file(const Run &r) {
     std::fprintf(fp, "# columns: 1 t, 2 a, 3 Etot, 4 Ekin, 5 Egrad, 6 Epot, 7-10 spread of Etot/Ekin/Egrad/Epot,\n");
     std::fprintf(fp, "#          11 <phi>, 12 spread of <phi>, 13 <phi'>, 14 spread of <phi'>, 15 H, 16 Hubble constraint C = H^2 - rho/(3 Mpl^2)\n");
     std::fclose(fp);
+    /* bubble.cpp:967-973 */
+    if (r.o.walltracking == 1) {
+        fp = std::fopen((r.folder + "/gamma.dat").c_str(), "w");
+        if (!fp) throw std::runtime_error("Could not open gamma.dat for writing");
+        std::fprintf(fp, "#t, gamma factor, wall width, rmin, rmax\n");
+        std::fclose(fp);
+    }
 }
 
 /* bubble.cpp:977-989: one line of the box averages */
@@ -171,7 +190,8 @@ void parameters_file(const Run &r) {
     std::fprintf(fp, "# The data in this folder correspond to the following:\n");
     std::fprintf(fp, " D = %d , L = %.10g,  nGrids = %d , TIME_STEP = %.10g  \n", o.D, o.L, o.nGrids, o.dt);
     std::fprintf(fp, " c = %.10g , nt = %d,  readxns = %d , expansion = %d  \n", o.c, o.nt, o.mode, o.expansion);
-    std::fprintf(fp, " nb = %d , FFT = %d,  ALPHAVAL = %d , WallTracking = %d  \n", o.nbubbles, 1, o.alpha, 0);
+    std::fprintf(fp, " nb = %d , FFT = %d,  ALPHAVAL = %d , WallTracking = %d  \n", o.nbubbles, 1, o.alpha,
+                 o.walltracking);
     std::fprintf(fp, "Mpl = %.10g, memorysave = %d, TEST = %d  \n", o.mpl, o.memorysave, o.test);
     std::fprintf(fp, " Full1DFieldEvery = %d , Trad = %.10g , fixedseed = %d \n", kFull1DFieldEvery, o.trad, 1);
     std::fprintf(fp, " kUV = %.10g , kIR = %.10g , kRStar = %.10g , kMeff = %.10g \n", kUV, kIR, kRStar, kMeff);
@@ -248,6 +268,97 @@ bool full_field(Run &r) {
     return true;
 }
 
+/* ---- wall tracking (bubble.cpp:535-634) ---------------------------------- */
+
+bool can_track_wall(const Options &o) { return o.D == 1 || o.mode == -1 || o.mode == -2; }
+
+/* first step of the tracking: half an oscillation period in the true vacuum */
+int wall_track_start(const Run &r) { return int(M_PI / r.wall.mT / r.o.dt); }
+
+void init_wall(Run &r) {
+    const Options &o = r.o;
+    Wall &w = r.wall;
+    w.rn = o.D == 3 ? 0.823 * std::pow(o.c, 0.203) * 1.3 : 0.823 * std::pow(o.c, 0.203);
+    w.lw = 0.496 * std::pow(o.c, -0.531);
+    w.phi_max = o.c / (6 + 2 * o.c);
+    w.phi_zero = (2 + o.c - std::sqrt(4 + o.c)) / (3 + o.c);
+    w.mT = std::sqrt(2 * (o.c + 6));
+    const int mid = o.D == 3 ? o.nGrids / 2 : 0;
+    if (o.mode == -2 && o.D >= 2) { w.centre[0] = o.nGrids / 2; w.centre[1] = o.nGrids / 2; w.centre[2] = mid; }
+    else if (o.mode == -1 && o.D >= 2) { w.centre[0] = o.nGrids / 4; w.centre[1] = o.nGrids / 4; w.centre[2] = mid; }
+}
+
+double gamma_factor(const Run &r, double d) {
+    if (r.o.walltracking == 0 || d == 0) return 0;
+    return r.wall.dini / d;
+}
+
+/* WallFinder (bubble.cpp:575-617): along axis 0 from the bubble centre, Rmin
+ * is the outermost radius where phi is still above its exit value, Rmax the
+ * first where it has dropped to the barrier top. The line comes from the
+ * device (cb_get_line); the search is the reference's, on the host. */
+bool wall_finder(Run &r) {
+    const Options &o = r.o;
+    Wall &w = r.wall;
+    const double dx = double(o.L) / o.nGrids;
+    const double maximal = (o.mode == -1 && o.D >= 2) ? o.L / 4.0 - o.deltar : o.L / 2.0;
+    if (w.rmax >= 0.98 * maximal || w.rmin >= 0.98 * maximal) {
+        std::cout << "bubble has almost left the box" << std::endl;
+        return true;
+    }
+    std::vector<double> line(o.nGrids);
+    const int st = cb_get_line(r.h, w.centre[0], w.centre[1], w.centre[2], o.nGrids, line.data());
+    if (st != CB_OK) return r.fail(st, "reading the wall line");
+    auto radius = [&](int i) { return dx * std::sqrt((i + 0.5) * (i + 0.5) + 0.25 * (o.D - 1)); };
+    const int istart = std::max(int((w.rmin - w.lw) / dx), int(w.rn / (2 * dx)));
+    w.rmin = 0;
+    w.rmax = 0;
+    for (int i = istart; (w.rmax == 0 || w.rmin == 0) && radius(i) < maximal; i++) {
+        const double v = line[(size_t)i % line.size()];
+        if (v > w.phi_zero) w.rmin = radius(i);
+        if (v <= w.phi_max && w.rmax == 0) w.rmax = radius(i);
+    }
+    if (w.rmax < w.rmin) {
+        std::cout << "Rmax < Rmin ! Something went wrong ... " << std::endl;
+        return true;
+    }
+    if (w.rmax * w.rmin == 0 && w.rmin + w.rmax != 0) w.rmax = w.rmin;
+    w.width = w.rmax - w.rmin;
+    std::cout << "WallWidth is: " << w.width << std::endl;
+    return true;
+}
+
+/* bubble.cpp:1009-1015 */
+void out_gamma(const Run &r) {
+    FILE *fp = std::fopen((r.folder + "/gamma.dat").c_str(), "a");
+    if (!fp) return;
+    std::fprintf(fp, "%.3f %.4f %.3f %.3f %.3f\n ", r.line.t, gamma_factor(r, r.wall.width), r.wall.width,
+                 r.wall.rmin, r.wall.rmax);
+    std::fclose(fp);
+}
+
+/* TrackWall (bubble.cpp:543-560) */
+bool track_wall(Run &r, int it) {
+    const int start = wall_track_start(r);
+    if (it == start) {
+        if (!wall_finder(r)) return false;
+        r.wall.dini = r.wall.width;
+        std::cout << "initial wall width: " << r.wall.dini << std::endl;
+        out_gamma(r);
+    } else if (it > start && it % kWallTrackEvery == 0 && r.line.t < r.o.L / 2) {
+        if (!wall_finder(r)) return false;
+        out_gamma(r);
+        std::cout << "gamma factor: " << gamma_factor(r, r.wall.width) << std::endl;
+    }
+    return true;
+}
+
+/* UpdateWall (bubble.cpp:569-573): the wall at a snapshot step */
+bool update_wall(Run &r, int it) {
+    if (it > wall_track_start(r) && r.line.t < r.o.L / 2) return wall_finder(r);
+    return true;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -307,6 +418,11 @@ int main(int argc, char **argv) {
 
     const std::vector<int> snaps = schedule(o);
     size_t next_snap = 0;
+    const bool track = o.walltracking == 1 && can_track_wall(o);
+    if (o.walltracking == 1 && !track)
+        std::cout << "Note: wall tracking only works in 1D or with --mode -1 or -2; skipping it." << std::endl;
+    init_wall(r);
+    const int wall_start = wall_track_start(r);
     const int progress = std::max(1, o.nt / 20);
     int it = 1;
     while (it <= o.nt) {
@@ -316,13 +432,20 @@ int main(int argc, char **argv) {
         if (next_snap < snaps.size()) next = std::min(next, snaps[next_snap]);
         if (o.D == 1) next = std::min(next, ((it + kFull1DFieldEvery - 1) / kFull1DFieldEvery) * kFull1DFieldEvery);
         next = std::min(next, ((it + progress - 1) / progress) * progress);
+        if (track) {
+            if (it <= wall_start) next = std::min(next, wall_start);
+            else next = std::min(next, ((it + kWallTrackEvery - 1) / kWallTrackEvery) * kWallTrackEvery);
+        }
         const bool snap = next_snap < snaps.size() && next == snaps[next_snap];
         st = cb_step(r.h, next - it + 1, CB_STEP_SUMS | (snap && o.memorysave == 0 ? CB_STEP_LOCAL : 0), &r.line);
         if (st != CB_OK) return r.fail(st, "stepping") ? 0 : 1;
         it = next + 1;
+        /* the reference's order within a step (main.cpp:276-285) */
+        if (track && !track_wall(r, next)) return 1;
         if (o.D == 1 && next % kFull1DFieldEvery == 0 && !full_field(r)) return 1;
         if (next % kOutEnergyEvery == 0) energy_line(r, r.line);
         if (snap) {
+            if (track && !update_wall(r, next)) return 1;
             if (!snapshot(r, (int)++next_snap)) return 1;
         }
         if (next % progress == 0)

@@ -152,6 +152,14 @@ int cb_get_fields(cb_handle *h, double *phi, double *pi, double *ekin, double *e
  * bubble.cpp:905-915), halving the bytes moved. */
 int cb_get_fields_f32(cb_handle *h, float *phi, float *pi, float *ekin, float *egrad, float *epot);
 
+/* One line of phi along lattice axis 0 through the site (i0, i1, i2):
+ * out[m] = phi[(i0 + m) mod n][i1][i2] for m = 0 .. count - 1 (i1 is ignored
+ * for d = 1, i2 for d <= 2), the field at the current time, count <= n.
+ * Replaces the wall finder's reads of Bubble::phi along the line from the
+ * tracked bubble's centre (bubble.cpp:588-592, phiAlong in WallFinder):
+ * only these values leave the device. */
+int cb_get_line(cb_handle *h, int i0, int i1, int i2, int count, double *out);
+
 /* Number of |k| shells: floor(sqrt(d) * n / 2) + 1 (bubble.hpp:49, bubble.cpp:671). */
 int cb_nbins(int d, int n_grids);
 

@@ -129,11 +129,52 @@ def run_dir():
                 shutil.copy(p, os.path.join(dst, fn))
 
 
+WALL_RUNS = {
+    # 1-D: the bubble at the box edge, wall tracked from step 112, FullField.dat every 100 steps
+    "run_d1_wall": dict(args=["--D", "1", "--nGrids", "512", "--L", "32", "--nt", "1300", "--c", "4",
+                              "--mode", "1", "--snapshots", "2"], dt=0.1 * 32.0 / 512),
+    # 2-D: one bubble in the centre (mode -2)
+    "run_d2_wall": dict(args=["--D", "2", "--nGrids", "128", "--L", "32", "--nt", "700", "--c", "4",
+                              "--mode", "-2", "--snapshots", "2"], dt=0.1 * 32.0 / 128),
+}
+
+
+def run_wall_dirs():
+    """Runs of the reference executable with wall tracking on (WallTracking = 1):
+    only the files that tracking and the 1-D line writer produce are kept."""
+    from oracle import bridge as B
+    B.build_reference()
+    for name, cfg in WALL_RUNS.items():
+        dst = os.path.join(HERE, name)
+        shutil.rmtree(dst, ignore_errors=True)
+        os.makedirs(dst)
+        with tempfile.TemporaryDirectory() as tmp:
+            env = dict(os.environ, CBREF_DT=repr(cfg["dt"]), CBREF_WALLTRACKING="1", OMP_NUM_THREADS="2")
+            args = [B.REF_EXE] + cfg["args"] + ["--no-plots", "--out", tmp]
+            out = subprocess.run(args, check=True, env=env, capture_output=True, text=True).stdout
+            (folder,) = os.listdir(tmp)
+            src = os.path.join(tmp, folder)
+            with open(os.path.join(dst, "folder_name.txt"), "w") as f:
+                f.write(folder + "\n")
+            with open(os.path.join(dst, "args.json"), "w") as f:
+                json.dump(dict(args=cfg["args"] + ["--no-plots"], dt=cfg["dt"]), f)
+            with open(os.path.join(dst, "stdout_wall.txt"), "w") as f:
+                f.writelines(ln + "\n" for ln in out.splitlines()
+                             if ln.startswith(("initial wall width", "WallWidth is", "gamma factor", "bubble has")))
+            for fn in ("gamma.dat", "FullField.dat"):
+                if os.path.exists(os.path.join(src, fn)):
+                    shutil.copy(os.path.join(src, fn), os.path.join(dst, fn))
+
+
 def main():
     from oracle import bridge as B
     B.build_reference()
     if len(sys.argv) > 2 and sys.argv[1] == "--case":
         one_case(sys.argv[2])
+        return
+    if len(sys.argv) > 1 and sys.argv[1] == "--wall":
+        run_wall_dirs()
+        print("wrote", ", ".join(WALL_RUNS))
         return
     for name in CASES:
         subprocess.run([sys.executable, __file__, "--case", name], check=True,
@@ -141,6 +182,8 @@ def main():
         print("wrote", name)
     run_dir()
     print("wrote run_d2/")
+    run_wall_dirs()
+    print("wrote", ", ".join(WALL_RUNS))
 
 
 if __name__ == "__main__":

@@ -94,3 +94,37 @@ def test_run_folder_matches_reference_executable():
                         assert float(x.split()[2]) == pytest.approx(float(y.split()[2]), rel=1e-14, abs=1e-300)
                     else:
                         assert x == y
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["run_d1_wall", "run_d2_wall"])
+def test_wall_tracking_matches_reference_executable(name):
+    """Wall tracking (--wall-tracking 1, the reference's WallTracking = 1):
+    gamma.dat, the wall messages on stdout and, in 1-D, FullField.dat against
+    the reference executable's own run (tests/golden/<name>)."""
+    gold = os.path.join(ROOT, "tests", "golden", name)
+    meta = json.load(open(os.path.join(gold, "args.json")))
+    with tempfile.TemporaryDirectory() as tmp:
+        r = run(meta["args"] + ["--dt", repr(meta["dt"]), "--wall-tracking", "1", "--out", tmp])
+        assert r.returncode == 0, r.stderr
+        (folder,) = os.listdir(tmp)
+        assert folder == open(os.path.join(gold, "folder_name.txt")).read().strip()
+        mine = os.path.join(tmp, folder)
+        ga, gb = open(os.path.join(mine, "gamma.dat")).read(), open(os.path.join(gold, "gamma.dat")).read()
+        assert ga.split("\n")[0] == gb.split("\n")[0]
+        A = [[float(x) for x in ln.split()] for ln in ga.split("\n")[1:] if ln.strip()]
+        B = [[float(x) for x in ln.split()] for ln in gb.split("\n")[1:] if ln.strip()]
+        assert len(A) == len(B) and len(B) >= 2
+        np.testing.assert_allclose(A, B, rtol=0, atol=1.5e-3)     # printed with 3-4 decimals
+        msgs = [ln for ln in r.stdout.splitlines()
+                if ln.startswith(("initial wall width", "WallWidth is", "gamma factor", "bubble has"))]
+        ref = open(os.path.join(gold, "stdout_wall.txt")).read().splitlines()
+        assert [m.split(":")[0] for m in msgs] == [m.split(":")[0] for m in ref]
+        for m, q in zip(msgs, ref):
+            if ":" in m:
+                assert float(m.split(":")[1]) == pytest.approx(float(q.split(":")[1]), rel=1e-5, abs=1e-5)
+        if os.path.exists(os.path.join(gold, "FullField.dat")):
+            A, B = _numbers(os.path.join(mine, "FullField.dat")), _numbers(os.path.join(gold, "FullField.dat"))
+            assert len(A) == len(B)
+            np.testing.assert_allclose(np.array(A), np.array(B), rtol=0, atol=1.5e-5)
+

@@ -287,3 +287,26 @@ def test_temporal_blocking_matches_single_step_passes(n, L, steps, tl, monkeypat
     for k, rk in (("etot", "Etot"), ("egrad", "Egradtot"), ("epot", "Epottot")):
         assert abs(a[k] - r[rk]) <= 1e-5 * abs(r[rk]), k
     assert a["t"] == b["t"] == r["t"]
+
+
+@pytest.mark.parametrize("case", [
+    dict(d=1, n=256, L=32.0, c=4.0, expansion=0, prec="fp64", start=(5, 0, 0)),
+    dict(d=2, n=96, L=24.0, c=3.0, expansion=0, prec="fp64", start=(70, 13, 0)),
+    dict(d=3, n=64, L=16.0, c=4.0, expansion=1, prec="fp64", start=(40, 7, 19)),    # a drift pending
+    dict(d=3, n=64, L=16.0, c=4.0, expansion=1, prec="fp32c", start=(3, 60, 1)),
+])
+def test_line_equals_the_field(case):
+    """cb_get_line (the wall finder's line) equals the same sites of the full
+    field bit for bit, including a run whose last drift is still pending."""
+    import coolbubble_b200 as cb
+    d, n, L, c = case["d"], case["n"], case["L"], case["c"]
+    p = cb.make_params(d, n, L, c, 0.1 * L / n, expansion=case["expansion"], mpl=10.0, precision=case["prec"])
+    s = cb.Bubble(p, bubbles(d, n, L, c, 4, seed=9), smooth_noise(d, n, 0.02, seed=2))
+    s.step(13, sums=False)
+    i0, i1, i2 = case["start"]
+    line = s.line(i0, i1, i2)
+    phi = s.fields(local=False)["phi"].reshape((n,) * d)
+    idx = [(i0 + m) % n for m in range(n)]
+    want = phi[idx] if d == 1 else (phi[idx, i1] if d == 2 else phi[idx, i1, i2])
+    np.testing.assert_array_equal(line, want)
+    np.testing.assert_array_equal(s.line(i0, i1, i2, count=7), want[:7])
