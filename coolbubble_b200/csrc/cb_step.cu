@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(TX *TY) k_step(StepConst k, const T *__restric
     }
 }
 
-/* ---- set-up kernels (once per run; plain global loads) ------------------ */
+/* ---- set-up kernels (once per run; plain global loads, through L1/L2) --- */
 
 __device__ __forceinline__ size_t nb_index(const StepConst &k, size_t s, int axis, int dir) {
     size_t stride = 1;
@@ -201,6 +201,36 @@ __device__ __forceinline__ size_t nb_index(const StepConst &k, size_t s, int axi
 template <typename T>
 __device__ __forceinline__ T load_as(const void *p, size_t i) { return static_cast<const T *>(p)[i]; }
 
+/* Periodic neighbours of site s for lattices of fewer than 2^32 sites: the
+ * coordinates are taken once per site (32-bit divisions), each neighbour is
+ * then an add or a wrap along its axis (axis 0 has the largest stride, as
+ * gridfuncs.cpp:25-51). */
+struct Site32 {
+    unsigned s, n;
+    unsigned c[3], stride[3];
+    int d;
+    __device__ __forceinline__ Site32(const StepConst &k, unsigned site) : s(site), n((unsigned)k.n), d(k.d) {
+        unsigned rest = site, st = 1;
+        for (int ax = 2; ax >= 0; --ax) {
+            if (ax < d) {
+                c[ax] = rest % n;
+                rest /= n;
+                stride[ax] = st;
+                st *= n;
+            } else {
+                c[ax] = 0;
+                stride[ax] = 0;
+            }
+        }
+    }
+    __device__ __forceinline__ unsigned plus(int ax) const {
+        return c[ax] + 1 == n ? s - c[ax] * stride[ax] : s + stride[ax];
+    }
+    __device__ __forceinline__ unsigned minus(int ax) const {
+        return c[ax] == 0 ? s + (n - 1) * stride[ax] : s - stride[ax];
+    }
+};
+
 /* Initial energies with forward differences over dx (bubble.cpp:239-269) and
  * the start of the background (271-276). */
 template <typename T, int NT>
@@ -211,12 +241,23 @@ __global__ void __launch_bounds__(NT) k_ic_energies(StepConst k, size_t N, const
 #pragma unroll
     for (int s = 0; s < NSUM; ++s) v[s] = 0.0;
     const double dx = k.dx;
+    const bool small = N < (1ull << 32);
     for (size_t s = blockIdx.x * (size_t)NT + threadIdx.x; s < N; s += (size_t)gridDim.x * NT) {
         const double f = (double)phi[s];
         double g2 = 0.0;
-        for (int ax = 0; ax < k.d; ++ax) {
-            const double g = __ddiv_rn(__dsub_rn((double)phi[nb_index(k, s, ax, +1)], f), dx);
-            g2 = __dadd_rn(g2, __dmul_rn(g, g));
+        if (small) {
+            const Site32 q(k, (unsigned)s);
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax)
+                if (ax < k.d) {
+                    const double g = __ddiv_rn(__dsub_rn((double)phi[q.plus(ax)], f), dx);
+                    g2 = __dadd_rn(g2, __dmul_rn(g, g));
+                }
+        } else {
+            for (int ax = 0; ax < k.d; ++ax) {
+                const double g = __ddiv_rn(__dsub_rn((double)phi[nb_index(k, s, ax, +1)], f), dx);
+                g2 = __dadd_rn(g2, __dmul_rn(g, g));
+            }
         }
         const double eg = __dmul_rn(0.5, g2);
         const double ep = Vpot<double>(k, f);
@@ -278,13 +319,24 @@ __global__ void __launch_bounds__(NT) k_ic_backkick(StepConst k, size_t N, const
     const double w = __dmul_rn(0.5, pow(a_mhalf, (double)(-2 * k.d)));
     const T fl = (T)pow(st->a, (double)(k.d - 2 + k.alpha)), fv = (T)pow(st->a, (double)(k.d + k.alpha));
     const T hdt = (T)__dmul_rn(0.5, k.dt);
+    const bool small = N < (1ull << 32);
     for (size_t s = blockIdx.x * (size_t)NT + threadIdx.x; s < N; s += (size_t)gridDim.x * NT) {
         const T f = phi[s];
         const T two = A::add(f, f);
         T lap = (T)0;
-        for (int ax = 0; ax < k.d; ++ax) {
-            const T t = A::add(A::sub(phi[nb_index(k, s, ax, +1)], two), phi[nb_index(k, s, ax, -1)]);
-            lap = ax == 0 ? t : A::add(lap, t);
+        if (small) {
+            const Site32 q(k, (unsigned)s);
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax)
+                if (ax < k.d) {
+                    const T t = A::add(A::sub(phi[q.plus(ax)], two), phi[q.minus(ax)]);
+                    lap = ax == 0 ? t : A::add(lap, t);
+                }
+        } else {
+            for (int ax = 0; ax < k.d; ++ax) {
+                const T t = A::add(A::sub(phi[nb_index(k, s, ax, +1)], two), phi[nb_index(k, s, ax, -1)]);
+                lap = ax == 0 ? t : A::add(lap, t);
+            }
         }
         const T flap = A::mul(fl, lap);
         const T force = A::sub(k.dx2_pow2 ? A::mul(flap, kc<T>(k.inv_dx2, k.inv_dx2f)) : A::div(flap, kc<T>(k.dx2, k.dx2f)),
