@@ -1,37 +1,37 @@
-/* cb_step3_tb.cu -- TL leapfrog steps per HBM pass on static 3-D lattices.
+/* cb_step3_tb.cu -- two leapfrog steps per HBM pass on static 3-D lattices.
  *
  * Temporal blocking of the step of cb_step3.cu (reference Bubble::oneStep,
- * src/bubble.cpp:849-876, static background: a = 1, so the drift factor is 1
- * and no step needs a global sum). One launch reads phi_n, pi_{n-1/2} and
- * writes phi_{n+TL}, pi_{n+TL-1/2}:
+ * src/bubble.cpp:849-876, static background: a = 1, no step between two
+ * reported ones needs a global sum). One launch reads phi_n, pi_{n-1/2} and
+ * writes phi_{n+2}, pi_{n+3/2}: half the DRAM bytes per step.
  *
- *  - A work item is a tile of TJ full rows of axis 1 (every site of axis 2,
- *    so axis-2 neighbours wrap inside shared memory) and a chunk of CZ output
- *    planes of axis 0.
- *  - Level 0 (the input) arrives by TMA bulk copies into an S-deep ring:
- *    phi on rows [j0 - TL, j0 + TJ + TL) and pi on [j0 - TL + 1, j0 + TJ + TL - 1)
- *    (periodic rows, one copy per halo row and one for the tile's block).
- *  - Level l (1..TL) covers rows [j0 - (TL - l), j0 + TJ + (TL - l)): one row
- *    less per side per level. Streaming along axis 0, level l runs l planes
- *    behind the newest input plane, so when input plane q lands, level l
- *    computes plane q - l from level l-1's planes q-l-1, q-l, q-l+1.
- *    Levels 1..TL-1 keep phi in a 3-plane ring and pi in a 2-plane ring in
- *    shared memory; level TL writes the tile's rows to HBM.
- *  - A chunk needs input planes [i0 - TL, i1 + TL): the 2 TL extra planes and
- *    the extra rows are recomputed by the neighbouring work items (overlapped
- *    tiling, no communication between blocks). Blocks are ordered chunk-fastest
- *    so the chunks of one tile run together and share boundary planes in L2.
- *  - One producer warp issues the copies; eight consumer warps compute; a
- *    consumer-only barrier separates the levels of one plane step. Waits are
- *    bounded (clock64) and a timed-out block records an error word.
- *
- * Float fields only (the FP32C path); per-site arithmetic is the same as the
- * single-step kernel's.
+ *  - Tiles of TJ full rows of axis 1 (axis-2 neighbours wrap in shared
+ *    memory); work items (plane part, tile) taken from a device-wide queue,
+ *    part-major with tiles fastest, one block per SM.
+ *  - Input planes arrive by TMA bulk copies into a ring: phi rows
+ *    [j0 - 2, j0 + TJ + 2), pi rows [j0 - 1, j0 + TJ + 1) (periodic rows).
+ *  - Level 1 (the first step) covers rows [j0 - 1, j0 + TJ + 1) and keeps
+ *    phi (all its rows) and pi (the tile's rows) in a 4-plane ring in shared
+ *    memory; level 2 (the second step) covers the tile's rows and writes phi
+ *    and pi to HBM.
+ *  - Streaming along axis 0: when input plane q has landed, level 1 computes
+ *    plane q - 1 and level 2 plane q - 3, from level-1 planes finished in
+ *    earlier rounds, so one consumer barrier per input plane separates the
+ *    levels and the two levels' work interleaves freely between barriers.
+ *  - An item computing planes [p0, p1) streams input planes p0 - 2 .. p1 + 1
+ *    (overlapped tiling: neighbouring items recompute the halo, no block
+ *    talks to another). The input ring runs on from one item to the next.
+ *  - Per-site arithmetic is the single-step kernel's float path (packed
+ *    f32x2, same operations in the same order), so two blocked steps give the
+ *    fields of two single steps bit for bit.
+ *  - Waits are bounded (clock64 limit, sleeping retries); a timed-out block
+ *    records an error word; consumer warps leave together (a vote in the
+ *    per-plane barrier).
  */
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <type_traits>
+#include <cstdlib>
 
 #include "cb_internal.h"
 #include "cb_step_common.cuh"
@@ -41,211 +41,305 @@ namespace cb {
 
 namespace {
 
-constexpr int TB_CW = 16;
+constexpr int TB_CW = 16;                 /* consumer warps */
 constexpr int TB_NC = TB_CW * 32;
-constexpr int TB_NT = TB_NC + 32;
-constexpr int TB_HDR = 256;
+constexpr int TB_NT = TB_NC + 32;         /* plus one producer warp */
+constexpr int TB_HDR = 256;               /* full[8], empty[8], item_full[TB_IQ] mbarriers */
+constexpr int TB_IQ = 8;
+constexpr int L1_SLOTS = 4;               /* level-1 planes kept */
 
-__device__ __forceinline__ void tb_consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(TB_NC) : "memory"); }
+/* consumer-only barrier (id 1) returning whether any consumer passed true */
+__device__ __forceinline__ bool tb_consumer_any(bool x) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, 1, %2, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)x), "n"(TB_NC)
+        : "memory");
+    return r != 0;
+}
 
-template <typename T, int TL>
+struct TbCursor {
+    int s;
+    uint32_t ph;
+    __device__ __forceinline__ void next(int nstage) {
+        if (++s == nstage) {
+            s = 0;
+            ph ^= 1u;
+        }
+    }
+};
+
+/* Packed constants of the static float update (a = 1). */
+struct Pk {
+    F2 fl, idx2, nfv, dt, c2, nc3, c4;
+};
+
+/* One 16-byte vector (sites kk .. kk+3 of one row) of one leapfrog step on the
+ * static background: pi' = pi + dt F(phi), phi' = phi + dt pi' (bubble.cpp:
+ * 716-743, 853-856, 867-870 with a = 1), as two packed pairs -- the operations
+ * and their order of the single-step kernel's packed path. */
+__device__ __forceinline__ void update4(const Pk &K, const float4 c, const float4 um, const float4 up, const float4 im,
+                                        const float4 ip, float left, float right, const float4 pv, float4 &phi_n,
+                                        float4 &pi_n) {
+    const F2 c01 = f2_pack(c.x, c.y), c23 = f2_pack(c.z, c.w);
+    const F2 km01 = f2_pack(left, c.x), mid = f2_pack(c.y, c.z), kp23 = f2_pack(c.w, right);
+    auto pair = [&](F2 cc, F2 umm, F2 upp, F2 imm, F2 ipp, F2 kmm, F2 kpp, F2 pp, F2 &phi2, F2 &pi2) {
+        const F2 two = f2_add(cc, cc);
+        const F2 t0 = f2_add(f2_sub(ipp, two), imm);
+        const F2 t1 = f2_add(f2_sub(upp, two), umm);
+        const F2 t2 = f2_add(f2_sub(kpp, two), kmm);
+        const F2 lap = f2_add(f2_add(t0, t1), t2);
+        const F2 h = f2_fma(cc, f2_fma(cc, K.c4, K.nc3), K.c2);
+        const F2 force = f2_fma(f2_mul(K.fl, lap), K.idx2, f2_mul(K.nfv, f2_mul(cc, h)));
+        pi2 = f2_fma(K.dt, force, pp);
+        phi2 = f2_fma(K.dt, pi2, cc);
+    };
+    F2 phi01, pi01, phi23, pi23;
+    pair(c01, f2_pack(um.x, um.y), f2_pack(up.x, up.y), f2_pack(im.x, im.y), f2_pack(ip.x, ip.y), km01, mid,
+         f2_pack(pv.x, pv.y), phi01, pi01);
+    pair(c23, f2_pack(um.z, um.w), f2_pack(up.z, up.w), f2_pack(im.z, im.w), f2_pack(ip.z, ip.w), mid, kp23,
+         f2_pack(pv.z, pv.w), phi23, pi23);
+    phi_n = make_float4(f2_lo(phi01), f2_hi(phi01), f2_lo(phi23), f2_hi(phi23));
+    pi_n = make_float4(f2_lo(pi01), f2_hi(pi01), f2_lo(pi23), f2_hi(pi23));
+}
+
 __global__ void __launch_bounds__(TB_NT, 1)
-    k_step3_tb(StepConst k, int tj, int nstage, int cz, const T *__restrict__ phi_in, const T *__restrict__ pi_in,
-               T *__restrict__ phi_out, T *__restrict__ pi_out, DevState *st) {
-    static_assert(std::is_same<T, float>::value, "the blocked pass is the float path");
+    k_step3_t2(StepConst k, int tj, int nstage, int parts, const float *__restrict__ phi_in,
+               const float *__restrict__ pi_in, float *__restrict__ phi_out, float *__restrict__ pi_out,
+               DevState *st) {
     constexpr int W = 4;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ int abort_flag;
     __shared__ int issued_count;
-    __shared__ int consumer_stop;   /* snapshot of abort_flag all consumers act on */
+    __shared__ int item_q[TB_IQ];
 
     const int n = k.n;
-    const int R0 = tj + 2 * TL;        /* level-0 phi rows */
-    const int R0p = tj + 2 * TL - 2;   /* level-0 pi rows */
-    const size_t stage_elems = (size_t)(R0 + R0p) * n;
+    const int R0 = tj + 4;                 /* input phi rows: j0 - 2 .. j0 + tj + 1 */
+    const int R0p = tj + 2;                /* input pi rows: j0 - 1 .. j0 + tj */
+    const int R1 = tj + 2;                 /* level-1 phi rows: j0 - 1 .. j0 + tj */
+    const int stage_n = (R0 + R0p) * n;    /* floats per input stage */
+    const int slot_n = (R1 + tj) * n;      /* floats per level-1 slot: phi rows, then the tile's pi rows */
     uint64_t *full = reinterpret_cast<uint64_t *>(smraw);
-    uint64_t *empty = full + 16;
-    T *ring0 = reinterpret_cast<T *>(smraw + TB_HDR);
-    T *levels = ring0 + (size_t)nstage * stage_elems;
-    /* level l (1..TL-1): phi ring [3][R_l][n], then pi ring [2][R_(l+1)][n] holding
-     * only the rows level l+1 reads (the centre R_l - 2 rows of level l) */
-    auto rows_of = [&](int l) { return tj + 2 * (TL - l); };
-    auto level_base = [&](int l) {
-        size_t off = 0;
-        for (int m = 1; m < l; ++m) off += (size_t)(3 * rows_of(m) + 2 * rows_of(m + 1)) * n;
-        return levels + off;
-    };
+    uint64_t *empty = full + 8;
+    uint64_t *item_full = full + 16;
+    float *ring = reinterpret_cast<float *>(smraw + TB_HDR);
+    float *l1 = ring + (size_t)nstage * stage_n;
 
-    const int nchunks = (n + cz - 1) / cz;
-    const int chunk = blockIdx.x % nchunks;
-    const int tile = blockIdx.x / nchunks;
-    const int j0 = tile * tj;
-    const int i0 = chunk * cz;
-    const int i1 = min(i0 + cz, n);
-    const int pbase = i0 - TL;                 /* first input plane */
-    const int count0 = i1 - i0 + 2 * TL;       /* input planes */
-    const size_t row_bytes = (size_t)n * sizeof(T);
+    const int ntiles = n / tj;
+    const int items = ntiles * parts;
+    const size_t row_bytes = (size_t)n * sizeof(float);
     const size_t plane = (size_t)n * n;
     const uint32_t tx_bytes = (uint32_t)((size_t)(R0 + R0p) * row_bytes);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    auto stage_of = [&](int p) { return (p - pbase) % nstage; };
-    auto parity_of = [&](int p) { return (uint32_t)(((p - pbase) / nstage) & 1); };
+    auto item_of = [&](int it, int &t, int &p0, int &p1) {
+        const int c = it / ntiles;
+        t = it % ntiles;
+        p0 = (int)((long long)c * n / parts);
+        p1 = (int)((long long)(c + 1) * n / parts);
+    };
 
     if (threadIdx.x == 0) {
         abort_flag = 0;
         issued_count = 0;
-        consumer_stop = 0;
         for (int s = 0; s < nstage; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], TB_CW);
         }
+        for (int s = 0; s < TB_IQ; ++s) mbar_init(&item_full[s], 1);
         fence_mbar_init();
     }
     __syncthreads();
 
     if (warp == TB_CW) {
-        /* ---- producer: input planes pbase .. pbase + count0 - 1 ---- */
+        /* ---- producer: each item's input planes p0 - 2 .. p1 + 1 ---- */
         if (lane == 0) {
+            TbCursor pc{0, 0u};
+            bool wrapped = false;
             int q = 0;
-            for (; q < count0; ++q) {
-                const int s = q % nstage;
-                const int use = q / nstage;
-                if (use > 0 && !mbar_wait(&empty[s], (uint32_t)((use - 1) & 1), WAIT_LIMIT)) {
-                    atomicExch(&abort_flag, 1);
-                    break;
+            bool ok = true;
+            int cur = (int)atomicAdd(&st->item_next, 1u);
+            for (int j = 0; ok; ++j) {
+                /* the ring keeps the producer within two items of the consumers */
+                item_q[j % TB_IQ] = cur < items ? cur : -1;
+                mbar_arrive(&item_full[j % TB_IQ]);
+                if (cur >= items) break;
+                int t, p0, p1;
+                item_of(cur, t, p0, p1);
+                const int j0 = t * tj;
+                for (int pl = p0 - 2; pl <= p1 + 1; ++pl, ++q) {
+                    if (wrapped && !mbar_wait(&empty[pc.s], pc.ph ^ 1u, WAIT_LIMIT)) {
+                        atomicExch(&abort_flag, 1);
+                        ok = false;
+                        break;
+                    }
+                    if (abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    const int pw = pl < 0 ? pl + n : (pl >= n ? pl - n : pl);
+                    float *dst = ring + (size_t)pc.s * stage_n;
+                    float *dpi = dst + (size_t)R0 * n;
+                    const float *gphi = phi_in + (size_t)pw * plane;
+                    const float *gpi = pi_in + (size_t)pw * plane;
+                    fence_proxy_async();
+                    mbar_arrive_expect_tx(&full[pc.s], tx_bytes);
+                    for (int e = 0; e < 2; ++e) {
+                        const int ra = (j0 - 2 + e + n) % n, rb = (j0 + tj + e) % n;
+                        bulk_g2s(dst + (size_t)e * n, gphi + (size_t)ra * n, (uint32_t)row_bytes, &full[pc.s]);
+                        bulk_g2s(dst + (size_t)(2 + tj + e) * n, gphi + (size_t)rb * n, (uint32_t)row_bytes,
+                                 &full[pc.s]);
+                    }
+                    bulk_g2s(dst + (size_t)2 * n, gphi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[pc.s]);
+                    bulk_g2s(dpi, gpi + (size_t)((j0 - 1 + n) % n) * n, (uint32_t)row_bytes, &full[pc.s]);
+                    bulk_g2s(dpi + n, gpi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[pc.s]);
+                    bulk_g2s(dpi + (size_t)(1 + tj) * n, gpi + (size_t)((j0 + tj) % n) * n, (uint32_t)row_bytes,
+                             &full[pc.s]);
+                    pc.next(nstage);
+                    if (pc.s == 0) wrapped = true;
                 }
-                if (abort_flag) break;
-                const int pw = ((pbase + q) % n + n) % n;
-                T *dst = ring0 + (size_t)s * stage_elems;
-                T *dpi = dst + (size_t)R0 * n;
-                const T *gphi = phi_in + (size_t)pw * plane;
-                const T *gpi = pi_in + (size_t)pw * plane;
-                fence_proxy_async();
-                mbar_arrive_expect_tx(&full[s], tx_bytes);
-                /* phi: TL rows above, the tile's block, TL rows below */
-                for (int t = 0; t < TL; ++t) {
-                    const int ra = ((j0 - TL + t) % n + n) % n;
-                    bulk_g2s(dst + (size_t)t * n, gphi + (size_t)ra * n, (uint32_t)row_bytes, &full[s]);
-                    const int rb = (j0 + tj + t) % n;
-                    bulk_g2s(dst + (size_t)(TL + tj + t) * n, gphi + (size_t)rb * n, (uint32_t)row_bytes, &full[s]);
-                }
-                bulk_g2s(dst + (size_t)TL * n, gphi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
-                /* pi: TL - 1 rows above, the block, TL - 1 rows below */
-                for (int t = 0; t < TL - 1; ++t) {
-                    const int ra = ((j0 - TL + 1 + t) % n + n) % n;
-                    bulk_g2s(dpi + (size_t)t * n, gpi + (size_t)ra * n, (uint32_t)row_bytes, &full[s]);
-                    const int rb = (j0 + tj + t) % n;
-                    bulk_g2s(dpi + (size_t)(TL - 1 + tj + t) * n, gpi + (size_t)rb * n, (uint32_t)row_bytes, &full[s]);
-                }
-                bulk_g2s(dpi + (size_t)(TL - 1) * n, gpi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
+                /* the next item is taken once this one is fully issued */
+                if (ok) cur = (int)atomicAdd(&st->item_next, 1u);
             }
             issued_count = q;
         }
     } else {
         /* ---- consumers ---- */
-        const T dt = kc<T>(k.dt, k.dtf);
-        const T fl = (T)st->fl, fv = (T)st->fv;
-        const T inv_dx2 = kc<T>(k.inv_dx2, k.inv_dx2f);
-        const int nvr = n / W;   /* vectors per row */
-        const int nvr_shift = (nvr & (nvr - 1)) == 0 ? __ffs(nvr) - 1 : -1;
-        auto acquire = [&](int p) -> bool {
-            const bool ok = abort_flag == 0 && mbar_wait(&full[stage_of(p)], parity_of(p), WAIT_LIMIT);
+        Pk K;
+        K.fl = f2_splat((float)st->fl);
+        K.idx2 = f2_splat(k.inv_dx2f);
+        K.nfv = f2_splat(-(float)st->fv);
+        K.dt = f2_splat(k.dtf);
+        K.c2 = f2_splat(k.c2f);
+        K.nc3 = f2_splat(-k.c3f);
+        K.c4 = f2_splat(k.c4f);
+        const int nvr = n / W;                     /* vectors per row */
+        const int V1 = R1 * nvr, V2 = tj * nvr;    /* vectors of level 1 and level 2 per plane */
+        const int row_step = TB_NC / nvr, vec_step = TB_NC % nvr;
+        const int r_first = threadIdx.x / nvr, kv_first = threadIdx.x % nvr;
+        auto acquire = [&](const TbCursor &c) -> bool {
+            const bool ok = abort_flag == 0 && mbar_wait(&full[c.s], c.ph, WAIT_LIMIT);
             if (!ok) atomicExch(&abort_flag, 1);
             return ok;
         };
-        /* rows of level s at plane p: phi and pi pointers (row 0 of that level's layout) */
-        auto phi_rows = [&](int s, int p) -> const T * {
-            if (s == 0) return ring0 + (size_t)stage_of(p) * stage_elems;
-            return level_base(s) + (size_t)((p - pbase) % 3) * rows_of(s) * n;
-        };
-        auto pi_rows = [&](int s, int p) -> const T * {
-            if (s == 0) return ring0 + (size_t)stage_of(p) * stage_elems + (size_t)R0 * n;
-            return level_base(s) + (size_t)3 * rows_of(s) * n + (size_t)((p - pbase) % 2) * rows_of(s + 1) * n;
-        };
-        /* one level: rows [0, rows_of(l)) of level l at plane p from level l-1 */
-        auto level = [&](int l, int p) {
-            const int s = l - 1;
-            const int Rl = rows_of(l);
-            const T *Sm = phi_rows(s, p - 1), *S0 = phi_rows(s, p), *Sp = phi_rows(s, p + 1);
-            const T *P0 = pi_rows(s, p);
-            /* pi of level l-1 holds exactly the rows level l computes (row r at r) */
-            const int prow_off = 0;
-            T *out_phi = nullptr, *out_pi = nullptr;
-            if (l < TL) {
-                out_phi = level_base(l) + (size_t)((p - pbase) % 3) * Rl * n;
-                out_pi = level_base(l) + (size_t)3 * Rl * n + (size_t)((p - pbase) % 2) * (Rl - 2) * n;
+        /* One step over `rows` rows: row r reads phi rows r, r + 1, r + 2 of the
+         * planes Sm, S0, Sp (centre row r + 1) and pi row r of P; writes phi row
+         * r of Dphi and pi row r of Dpi (Dpi rows shifted by dpi_shift, rows
+         * outside [0, dpi_rows) not stored). */
+        auto level = [&](int nv, const float *Sm, const float *S0, const float *Sp, const float *P, float *Dphi,
+                         size_t dphi_stride_row, float *Dpi, int dpi_shift, int dpi_rows) {
+            int r = r_first, kv = kv_first;
+            for (int v = threadIdx.x; v < nv; v += TB_NC, r += row_step, kv += vec_step) {
+                if (kv >= nvr) {
+                    kv -= nvr;
+                    ++r;
+                }
+                const int kk = kv * W;
+                const int c_off = (r + 1) * n + kk;
+                const float4 c = *reinterpret_cast<const float4 *>(S0 + c_off);
+                const float4 um = *reinterpret_cast<const float4 *>(S0 + c_off - n);
+                const float4 up = *reinterpret_cast<const float4 *>(S0 + c_off + n);
+                const float4 im = *reinterpret_cast<const float4 *>(Sm + c_off);
+                const float4 ip = *reinterpret_cast<const float4 *>(Sp + c_off);
+                const float4 pv = *reinterpret_cast<const float4 *>(P + r * n + kk);
+                const float left = S0[(r + 1) * n + (kk == 0 ? n - 1 : kk - 1)];
+                const float right = S0[(r + 1) * n + (kk + W == n ? 0 : kk + W)];
+                float4 phi_n, pi_n;
+                update4(K, c, um, up, im, ip, left, right, pv, phi_n, pi_n);
+                *reinterpret_cast<float4 *>(Dphi + (size_t)r * dphi_stride_row + kk) = phi_n;
+                const int rp = r - dpi_shift;
+                if (rp >= 0 && rp < dpi_rows) *reinterpret_cast<float4 *>(Dpi + (size_t)rp * dphi_stride_row + kk) = pi_n;
             }
-            const int nv = Rl * nvr;
-            /* packed-pair constants: force = (fl inv_dx2) lap - fv V'(phi),
-             * V'(f) = f (c2 + f (-c3 + f c4)) */
-            const F2 FLX = f2_splat((float)(fl * inv_dx2)), NFV = f2_splat(-(float)fv), DT = f2_splat((float)dt);
-            const F2 C2 = f2_splat(k.c2f), NC3 = f2_splat(-k.c3f), C4 = f2_splat(k.c4f);
-            for (int v = threadIdx.x; v < nv; v += TB_NC) {
-                const int r = nvr_shift >= 0 ? (v >> nvr_shift) : v / nvr;
-                const int kk = (v - r * nvr) * W;
-                const size_t c_off = (size_t)(r + 1) * n + kk;
-                /* each 16-byte vector as two packed pairs (sites kk, kk+1) and (kk+2, kk+3) */
-                const ulonglong2 c = *reinterpret_cast<const ulonglong2 *>(S0 + c_off);
-                const ulonglong2 um = *reinterpret_cast<const ulonglong2 *>(S0 + c_off - n);
-                const ulonglong2 up = *reinterpret_cast<const ulonglong2 *>(S0 + c_off + n);
-                const ulonglong2 im = *reinterpret_cast<const ulonglong2 *>(Sm + c_off);
-                const ulonglong2 ip = *reinterpret_cast<const ulonglong2 *>(Sp + c_off);
-                const ulonglong2 pv = *reinterpret_cast<const ulonglong2 *>(P0 + (size_t)(r + prow_off) * n + kk);
-                const float left = S0[(size_t)(r + 1) * n + (kk == 0 ? n - 1 : kk - 1)];
-                const float right = S0[(size_t)(r + 1) * n + (kk + W == n ? 0 : kk + W)];
-                const F2 c01{c.x}, c23{c.y};
-                const F2 km01 = f2_pack(left, f2_lo(c01)), km23 = f2_pack(f2_hi(c01), f2_lo(c23));
-                const F2 kp01 = f2_pack(f2_hi(c01), f2_lo(c23)), kp23 = f2_pack(f2_hi(c23), right);
-                auto site2 = [&](F2 cc, F2 umm, F2 upp, F2 imm, F2 ipp, F2 kmm, F2 kpp, F2 pp, F2 &phi_n, F2 &pi_n) {
-                    const F2 two = f2_add(cc, cc);
-                    const F2 t0 = f2_add(f2_sub(ipp, two), imm);
-                    const F2 t1 = f2_add(f2_sub(upp, two), umm);
-                    const F2 t2 = f2_add(f2_sub(kpp, two), kmm);
-                    const F2 lap = f2_add(f2_add(t0, t1), t2);
-                    const F2 h = f2_fma(cc, f2_fma(cc, C4, NC3), C2);
-                    const F2 force = f2_fma(NFV, f2_mul(cc, h), f2_mul(lap, FLX));
-                    pi_n = f2_fma(DT, force, pp);
-                    phi_n = f2_fma(DT, pi_n, cc);
-                };
-                F2 phi01, pi01, phi23, pi23;
-                site2(c01, F2{um.x}, F2{up.x}, F2{im.x}, F2{ip.x}, km01, kp01, F2{pv.x}, phi01, pi01);
-                site2(c23, F2{um.y}, F2{up.y}, F2{im.y}, F2{ip.y}, km23, kp23, F2{pv.y}, phi23, pi23);
-                const ulonglong2 phi_new = make_ulonglong2(phi01.v, phi23.v);
-                const ulonglong2 pi_new = make_ulonglong2(pi01.v, pi23.v);
-                if (l < TL) {
-                    *reinterpret_cast<ulonglong2 *>(out_phi + (size_t)r * n + kk) = phi_new;
-                    if (r >= 1 && r < Rl - 1)
-                        *reinterpret_cast<ulonglong2 *>(out_pi + (size_t)(r - 1) * n + kk) = pi_new;
-                } else {
-                    const size_t o = ((size_t)p * n + j0 + r) * n + kk;
-                    *reinterpret_cast<ulonglong2 *>(pi_out + o) = pi_new;
-                    *reinterpret_cast<ulonglong2 *>(phi_out + o) = phi_new;
+        };
+        bool run = true;
+        TbCursor cq{0, 0u};   /* input cursor of the item's first plane */
+        for (int j = 0; run; ++j) {
+            if (abort_flag != 0 || !mbar_wait(&item_full[j % TB_IQ], (uint32_t)((j / TB_IQ) & 1), WAIT_LIMIT)) {
+                atomicExch(&abort_flag, 1);
+                run = false;
+            }
+            if (tb_consumer_any(!run)) {
+                run = false;
+                break;
+            }
+            const int it = item_q[j % TB_IQ];
+            if (it < 0) break;
+            int t, p0, p1;
+            item_of(it, t, p0, p1);
+            const int j0 = t * tj;
+            /* input cursors of planes q - 2, q - 1, q (q: the newest input plane) */
+            TbCursor ca = cq, cb = cq, cc = cq;
+            bool bad = false;
+            for (int q = p0 - 2; q <= p1 + 2; ++q) {
+                if (q <= p1 + 1) {
+                    /* advance the window to input plane q */
+                    if (q == p0 - 2) {
+                        cc = cq;
+                    } else {
+                        ca = cb;
+                        cb = cc;
+                        cc.next(nstage);
+                    }
+                    if (!bad && !acquire(cc)) bad = true;
+                }
+                if (!bad) {
+                    /* level 1 at plane q - 1 from input planes q - 2 .. q */
+                    if (q - 1 >= p0 - 1 && q - 1 <= p1 && q <= p1 + 1) {
+                        const float *Sm = ring + (size_t)ca.s * stage_n;
+                        const float *S0 = ring + (size_t)cb.s * stage_n;
+                        const float *Sp = ring + (size_t)cc.s * stage_n;
+                        float *D = l1 + (size_t)((q - 1 - (p0 - 1)) % L1_SLOTS) * slot_n;
+                        level(V1, Sm, S0, Sp, S0 + (size_t)R0 * n, D, n, D + (size_t)R1 * n, 1, tj);
+                    }
+                    /* level 2 at plane q - 3 from level-1 planes q - 4 .. q - 2 */
+                    const int p = q - 3;
+                    if (p >= p0 && p < p1) {
+                        const float *Lm = l1 + (size_t)((p - 1 - (p0 - 1)) % L1_SLOTS) * slot_n;
+                        const float *L0 = l1 + (size_t)((p - (p0 - 1)) % L1_SLOTS) * slot_n;
+                        const float *Lp = l1 + (size_t)((p + 1 - (p0 - 1)) % L1_SLOTS) * slot_n;
+                        const size_t g = ((size_t)p * n + j0) * n;
+                        level(V2, Lm, L0, Lp, L0 + (size_t)R1 * n, phi_out + g, n, pi_out + g, 0, tj);
+                    }
+                }
+                /* input plane q - 2 has had its last use (level 1 at plane q - 1);
+                 * the round after the last input plane only runs level 2 */
+                if (q >= p0 && q <= p1 + 1 && !bad) {
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&empty[ca.s]);
+                }
+                if (tb_consumer_any(bad)) {
+                    run = false;
+                    break;
                 }
             }
-        };
-        bool ok = acquire(pbase) && acquire(pbase + 1);
-        for (int q = pbase + 2; q < pbase + count0; ++q) {
-            ok = ok && acquire(q);
-            for (int l = 1; l <= TL; ++l) {
-                const int p = q - l;
-                if (ok && p >= i0 - (TL - l) && p < i1 + (TL - l)) level(l, p);
-                tb_consumer_sync();
-                if (l == 1) {
-                    /* input plane q - 2 has had its last use (level 1 at plane q - 1) */
-                    if (lane == 0) mbar_arrive(&empty[stage_of(q - 2)]);
-                    if (threadIdx.x == 0) consumer_stop = abort_flag;
-                }
+            if (!run) break;
+            /* the item's last two input planes p1 and p1 + 1 (under cb, cc) */
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&empty[cb.s]);
+                mbar_arrive(&empty[cc.s]);
             }
-            if (consumer_stop) break;
+            cq = cc;
+            cq.next(nstage);
         }
     }
     __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&st->item_done, 1u) == gridDim.x - 1) {
+            st->item_next = 0u;
+            st->item_done = 0u;
+        }
+    }
     if (abort_flag) {
         if (threadIdx.x == 0) {
             atomicExch(&st->err, ERR_TMA_TIMEOUT);
             const int q1 = issued_count;
             for (int q = q1 > nstage ? q1 - nstage : 0; q < q1; ++q)
-                mbar_wait(&full[stage_of(pbase + q)], parity_of(pbase + q), WAIT_LIMIT / 8);
+                mbar_wait(&full[q % nstage], (uint32_t)((q / nstage) & 1), WAIT_LIMIT / 8);
         }
         __syncthreads();
     }
@@ -253,54 +347,61 @@ __global__ void __launch_bounds__(TB_NT, 1)
 
 }  // namespace
 
-/* Geometry of the TL-step pass: float fields, d = 3, static background,
- * n a multiple of 4 in [64, 1024]. TJ rows with TJ * n about 2048 sites;
- * shared memory = 4-stage input ring + the level rings, one block per SM. */
+int sm_count();
+
+/* Geometry of the two-step pass: float fields, d = 3, static background,
+ * n a multiple of 4 in [64, 1024]. TJ rows with TJ * n about 2048 sites (4
+ * at 512^3, 8 at 256^3); shared memory = the input ring (4..6 stages) + the
+ * 4 level-1 planes, one block per SM; the number of plane parts balances an
+ * item's fixed cost (its 4 halo input planes, 2 extra level-1 planes) against
+ * a part-filled last round. */
 bool step3tb_geometry(const StepConst &k, int prec, int tl, int &tj, int &nstage, size_t &smem, unsigned &grid,
-                      int &cz) {
-    if (k.d != 3 || prec != P_FP32 || k.expanding || (tl != 2 && tl != 3)) return false;
+                      int &parts) {
+    if (k.d != 3 || prec != P_FP32 || k.expanding || tl != 2) return false;
     const int n = k.n;
     if (n % 4 != 0 || n < 64 || n > 1024) return false;
     const size_t esz = 4;
-    const size_t budget = 225 * 1024;   /* one block per SM: the input ring gets what the levels leave */
-    for (int target = 2048; target >= 256; target /= 2) {
-        tj = 1;
-        for (int t = 1; t <= n && t * n <= target; ++t)
-            if (n % t == 0) tj = t;
-        const size_t stage = (size_t)(2 * tj + 4 * tl - 2) * n * esz;
-        size_t lev = 0;
-        for (int l = 1; l < tl; ++l) lev += (size_t)(3 * (tj + 2 * (tl - l)) + 2 * (tj + 2 * (tl - l - 1))) * n * esz;
-        nstage = (int)((budget - TB_HDR - lev) / stage);
-        if (nstage > 8) nstage = 8;
-        smem = TB_HDR + (size_t)nstage * stage + lev;
-        if (nstage >= 5 && smem <= budget) break;
+    const size_t budget = 225 * 1024;
+    tj = 1;
+    for (int t = 1; t <= n && t * n <= 2048; ++t)
+        if (n % t == 0) tj = t;
+    const size_t stage = (size_t)(2 * tj + 6) * n * esz;
+    const size_t lev = (size_t)L1_SLOTS * (2 * tj + 2) * n * esz;
+    if (budget < TB_HDR + lev + 4 * stage) return false;
+    nstage = (int)((budget - TB_HDR - lev) / stage);
+    if (nstage > 6) nstage = 6;
+    smem = TB_HDR + (size_t)nstage * stage + lev;
+    const long long ntiles = n / tj;
+    const long long slots = sm_count();
+    const double fixed = 3.0;
+    double best = 1e300;
+    parts = 1;
+    for (int P = 1; P <= n / 4; ++P) {
+        const double per_item = (double)n / P + fixed;
+        const long long nitems = ntiles * P;
+        const double cost = nitems <= slots ? per_item : (double)nitems / slots * per_item + 0.5 * per_item;
+        if (cost < best - 1e-9) {
+            best = cost;
+            parts = P;
+        }
     }
-    if (nstage < 5 || smem > budget) return false;
-    const int ntiles = n / tj;
-    cz = 32;
-    while (cz > 8 && (size_t)ntiles * ((n + cz - 1) / cz) < 4 * 148) cz /= 2;
-    grid = (unsigned)(ntiles * ((n + cz - 1) / cz));
+    const char *env = std::getenv("CB_STEP3TB_PARTS");
+    if (env && std::atoi(env) >= 1 && std::atoi(env) <= n) parts = std::atoi(env);
+    const long long nitems = ntiles * parts;
+    grid = (unsigned)(nitems < slots ? nitems : slots);
     return true;
 }
 
 cudaError_t launch_step3_tb(int prec, const StepConst &k, int tl, const void *phi_in, const void *pi_in,
                             void *phi_out, void *pi_out, DevState *st, cudaStream_t s) {
-    int tj, nstage, cz;
+    int tj, nstage, parts;
     size_t smem;
     unsigned grid;
-    if (!step3tb_geometry(k, prec, tl, tj, nstage, smem, grid, cz)) return cudaErrorInvalidValue;
-    cudaError_t e;
-    if (tl == 2) {
-        e = cudaFuncSetAttribute(k_step3_tb<float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        k_step3_tb<float, 2><<<grid, TB_NT, smem, s>>>(k, tj, nstage, cz, (const float *)phi_in,
-                                                        (const float *)pi_in, (float *)phi_out, (float *)pi_out, st);
-    } else {
-        e = cudaFuncSetAttribute(k_step3_tb<float, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        k_step3_tb<float, 3><<<grid, TB_NT, smem, s>>>(k, tj, nstage, cz, (const float *)phi_in,
-                                                        (const float *)pi_in, (float *)phi_out, (float *)pi_out, st);
-    }
+    if (!step3tb_geometry(k, prec, tl, tj, nstage, smem, grid, parts)) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(k_step3_t2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_step3_t2<<<grid, TB_NT, smem, s>>>(k, tj, nstage, parts, (const float *)phi_in, (const float *)pi_in,
+                                        (float *)phi_out, (float *)pi_out, st);
     return cudaGetLastError();
 }
 

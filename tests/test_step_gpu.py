@@ -257,16 +257,22 @@ def test_device_error_word_stays_clear():
     assert s.device_error() == 0
 
 
-@pytest.mark.parametrize("n,L,steps", [(64, 16.0, 41), (96, 24.0, 40), (128, 32.0, 40), (256, 32.0, 80)])
-@pytest.mark.parametrize("tl", [2, 3])
+@pytest.mark.parametrize("n,L,steps", [(64, 16.0, 41), (96, 24.0, 40), (128, 32.0, 40), (256, 32.0, 80),
+                                       (512, 64.0, 9)])
+@pytest.mark.parametrize("tl", [2])
 def test_temporal_blocking_matches_single_step_passes(n, L, steps, tl, monkeypatch):
-    """Static float 3-D runs: TL steps per HBM pass give the same fields as one
-    step per pass (to float rounding) and energies within the FP32C bar."""
+    """Static float 3-D runs: two steps per HBM pass give the fields of one
+    step per pass bit for bit (same per-site arithmetic) and energies within
+    the FP32C bar."""
     import coolbubble_b200 as cb
     from oracle import bridge as B
     d, c = 3, 2.0
     dt = 0.1 * L / n
-    phi0, pi0 = smooth_noise(d, n, 0.3, seed=31), smooth_noise(d, n, 0.05, seed=32)
+    if n > 256:                         # white noise: the band-limited field's 512^3 FFT is slow on the host
+        rng = np.random.default_rng(31)
+        phi0, pi0 = 0.3 * rng.random(n ** d), 0.05 * rng.standard_normal(n ** d)
+    else:
+        phi0, pi0 = smooth_noise(d, n, 0.3, seed=31), smooth_noise(d, n, 0.05, seed=32)
     p = cb.make_params(d, n, L, c, dt, precision="fp32c", memorysave=1)
     monkeypatch.setenv("CB_TEMPORAL_BLOCK", str(tl))
     blocked = cb.Bubble(p, phi0, pi0)
@@ -280,7 +286,10 @@ def test_temporal_blocking_matches_single_step_passes(n, L, steps, tl, monkeypat
     assert single.counters() == (steps, steps)
     fa, fb = blocked.fields(local=False), single.fields(local=False)
     for k in ("phi", "pi"):
-        assert np.abs(fa[k] - fb[k]).max() <= 1e-5 * np.abs(fb[k]).max(), k
+        np.testing.assert_array_equal(fa[k], fb[k])
+    assert a == b
+    if n > 256:
+        return                          # the oracle's CPU run is the slow part; 512^3 checks the kernel only
     o = B.Oracle(d, n, L, c, dt, phi0, pi0)
     o.step(steps)
     r = o.scalars()
