@@ -41,15 +41,14 @@ namespace cb {
 
 namespace {
 
-constexpr int TB_CW = 16;                 /* consumer warps */
-constexpr int TB_NC = TB_CW * 32;
-constexpr int TB_NT = TB_NC + 32;         /* plus one producer warp */
+constexpr int TB_MAXT = 704;             /* at most 21 consumer warps + the producer warp */
 constexpr int TB_HDR = 256;               /* full[8], empty[8], item_full[TB_IQ] mbarriers */
 constexpr int TB_IQ = 8;
 constexpr int L1_SLOTS = 4;               /* level-1 planes kept */
 
-/* consumer-only barrier (id 1) returning whether any consumer passed true */
-__device__ __forceinline__ bool tb_consumer_any(bool x) {
+/* consumer-only barrier (id 1) over nc threads, returning whether any of
+ * them passed true */
+__device__ __forceinline__ bool tb_consumer_any(bool x, int nc) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
@@ -57,7 +56,7 @@ __device__ __forceinline__ bool tb_consumer_any(bool x) {
         "bar.red.or.pred p, 1, %2, q;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(r)
-        : "r"((uint32_t)x), "n"(TB_NC)
+        : "r"((uint32_t)x), "r"(nc)
         : "memory");
     return r != 0;
 }
@@ -107,7 +106,7 @@ __device__ __forceinline__ void update4(const Pk &K, const float4 c, const float
     pi_n = make_float4(f2_lo(pi01), f2_hi(pi01), f2_lo(pi23), f2_hi(pi23));
 }
 
-__global__ void __launch_bounds__(TB_NT, 1)
+__global__ void __launch_bounds__(TB_MAXT, 1)
     k_step3_t2(StepConst k, int tj, int nstage, int parts, const float *__restrict__ phi_in,
                const float *__restrict__ pi_in, float *__restrict__ phi_out, float *__restrict__ pi_out,
                DevState *st) {
@@ -135,6 +134,10 @@ __global__ void __launch_bounds__(TB_NT, 1)
     const size_t plane = (size_t)n * n;
     const uint32_t tx_bytes = (uint32_t)((size_t)(R0 + R0p) * row_bytes);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    /* consumer warps: all but the last warp of the block (the count is chosen
+     * on the host so that each consumer thread gets the same number of
+     * vectors per input plane) */
+    const int NC = blockDim.x - 32, CW = NC / 32;
     auto item_of = [&](int it, int &t, int &p0, int &p1) {
         const int c = it / ntiles;
         t = it % ntiles;
@@ -147,14 +150,14 @@ __global__ void __launch_bounds__(TB_NT, 1)
         issued_count = 0;
         for (int s = 0; s < nstage; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], TB_CW);
+            mbar_init(&empty[s], CW);
         }
         for (int s = 0; s < TB_IQ; ++s) mbar_init(&item_full[s], 1);
         fence_mbar_init();
     }
     __syncthreads();
 
-    if (warp == TB_CW) {
+    if (warp == CW) {
         /* ---- producer: each item's input planes p0 - 2 .. p1 + 1 ---- */
         if (lane == 0) {
             TbCursor pc{0, 0u};
@@ -218,40 +221,44 @@ __global__ void __launch_bounds__(TB_NT, 1)
         K.c4 = f2_splat(k.c4f);
         const int nvr = n / W;                     /* vectors per row */
         const int V1 = R1 * nvr, V2 = tj * nvr;    /* vectors of level 1 and level 2 per plane */
-        const int row_step = TB_NC / nvr, vec_step = TB_NC % nvr;
-        const int r_first = threadIdx.x / nvr, kv_first = threadIdx.x % nvr;
+        const int nvr_shift = (nvr & (nvr - 1)) == 0 ? __ffs(nvr) - 1 : -1;
         auto acquire = [&](const TbCursor &c) -> bool {
             const bool ok = abort_flag == 0 && mbar_wait(&full[c.s], c.ph, WAIT_LIMIT);
             if (!ok) atomicExch(&abort_flag, 1);
             return ok;
         };
-        /* One step over `rows` rows: row r reads phi rows r, r + 1, r + 2 of the
-         * planes Sm, S0, Sp (centre row r + 1) and pi row r of P; writes phi row
-         * r of Dphi and pi row r of Dpi (Dpi rows shifted by dpi_shift, rows
-         * outside [0, dpi_rows) not stored). */
-        auto level = [&](int nv, const float *Sm, const float *S0, const float *Sp, const float *P, float *Dphi,
-                         size_t dphi_stride_row, float *Dpi, int dpi_shift, int dpi_rows) {
-            int r = r_first, kv = kv_first;
-            for (int v = threadIdx.x; v < nv; v += TB_NC, r += row_step, kv += vec_step) {
-                if (kv >= nvr) {
-                    kv -= nvr;
-                    ++r;
-                }
-                const int kk = kv * W;
+        /* One round: vectors [0, n1) are level 1 (rows j0 - 1 .. j0 + tj of the
+         * planes under the input cursors, into level-1 slot D1), vectors
+         * [n1, n1 + n2) level 2 (the tile's rows from level-1 slots Lm, L0, Lp,
+         * into HBM at g). Row r of a level reads phi rows r, r + 1, r + 2 of its
+         * source planes (centre row r + 1) and pi row r. */
+        auto round = [&](int n1, const float *Sm, const float *S0, const float *Sp, float *D1, int n2,
+                         const float *Lm, const float *L0, const float *Lp, size_t g) {
+            for (int v = threadIdx.x; v < n1 + n2; v += NC) {
+                const bool one = v < n1;
+                const int u = one ? v : v - n1;
+                const int r = nvr_shift >= 0 ? (u >> nvr_shift) : u / nvr;
+                const int kk = (u - r * nvr) * W;
+                const float *A = one ? Sm : Lm, *B = one ? S0 : L0, *C = one ? Sp : Lp;
+                const float *P = B + (one ? R0 : R1) * n;
                 const int c_off = (r + 1) * n + kk;
-                const float4 c = *reinterpret_cast<const float4 *>(S0 + c_off);
-                const float4 um = *reinterpret_cast<const float4 *>(S0 + c_off - n);
-                const float4 up = *reinterpret_cast<const float4 *>(S0 + c_off + n);
-                const float4 im = *reinterpret_cast<const float4 *>(Sm + c_off);
-                const float4 ip = *reinterpret_cast<const float4 *>(Sp + c_off);
+                const float4 c = *reinterpret_cast<const float4 *>(B + c_off);
+                const float4 um = *reinterpret_cast<const float4 *>(B + c_off - n);
+                const float4 up = *reinterpret_cast<const float4 *>(B + c_off + n);
+                const float4 im = *reinterpret_cast<const float4 *>(A + c_off);
+                const float4 ip = *reinterpret_cast<const float4 *>(C + c_off);
                 const float4 pv = *reinterpret_cast<const float4 *>(P + r * n + kk);
-                const float left = S0[(r + 1) * n + (kk == 0 ? n - 1 : kk - 1)];
-                const float right = S0[(r + 1) * n + (kk + W == n ? 0 : kk + W)];
+                const float left = B[(r + 1) * n + (kk == 0 ? n - 1 : kk - 1)];
+                const float right = B[(r + 1) * n + (kk + W == n ? 0 : kk + W)];
                 float4 phi_n, pi_n;
                 update4(K, c, um, up, im, ip, left, right, pv, phi_n, pi_n);
-                *reinterpret_cast<float4 *>(Dphi + (size_t)r * dphi_stride_row + kk) = phi_n;
-                const int rp = r - dpi_shift;
-                if (rp >= 0 && rp < dpi_rows) *reinterpret_cast<float4 *>(Dpi + (size_t)rp * dphi_stride_row + kk) = pi_n;
+                if (one) {
+                    *reinterpret_cast<float4 *>(D1 + r * n + kk) = phi_n;
+                    if (r >= 1 && r <= tj) *reinterpret_cast<float4 *>(D1 + (R1 + r - 1) * n + kk) = pi_n;
+                } else {
+                    *reinterpret_cast<float4 *>(phi_out + g + (size_t)r * n + kk) = phi_n;
+                    *reinterpret_cast<float4 *>(pi_out + g + (size_t)r * n + kk) = pi_n;
+                }
             }
         };
         bool run = true;
@@ -261,7 +268,7 @@ __global__ void __launch_bounds__(TB_NT, 1)
                 atomicExch(&abort_flag, 1);
                 run = false;
             }
-            if (tb_consumer_any(!run)) {
+            if (tb_consumer_any(!run, NC)) {
                 run = false;
                 break;
             }
@@ -286,23 +293,18 @@ __global__ void __launch_bounds__(TB_NT, 1)
                     if (!bad && !acquire(cc)) bad = true;
                 }
                 if (!bad) {
-                    /* level 1 at plane q - 1 from input planes q - 2 .. q */
-                    if (q - 1 >= p0 - 1 && q - 1 <= p1 && q <= p1 + 1) {
-                        const float *Sm = ring + (size_t)ca.s * stage_n;
-                        const float *S0 = ring + (size_t)cb.s * stage_n;
-                        const float *Sp = ring + (size_t)cc.s * stage_n;
-                        float *D = l1 + (size_t)((q - 1 - (p0 - 1)) % L1_SLOTS) * slot_n;
-                        level(V1, Sm, S0, Sp, S0 + (size_t)R0 * n, D, n, D + (size_t)R1 * n, 1, tj);
-                    }
-                    /* level 2 at plane q - 3 from level-1 planes q - 4 .. q - 2 */
+                    /* level 1 at plane q - 1 from input planes q - 2 .. q; level 2
+                     * at plane p = q - 3 from level-1 planes p - 1 .. p + 1 (level-1
+                     * plane m sits in slot (m - p0 + 1) mod 4) */
+                    const bool do1 = q - 1 >= p0 - 1 && q - 1 <= p1 && q <= p1 + 1;
                     const int p = q - 3;
-                    if (p >= p0 && p < p1) {
-                        const float *Lm = l1 + (size_t)((p - 1 - (p0 - 1)) % L1_SLOTS) * slot_n;
-                        const float *L0 = l1 + (size_t)((p - (p0 - 1)) % L1_SLOTS) * slot_n;
-                        const float *Lp = l1 + (size_t)((p + 1 - (p0 - 1)) % L1_SLOTS) * slot_n;
-                        const size_t g = ((size_t)p * n + j0) * n;
-                        level(V2, Lm, L0, Lp, L0 + (size_t)R1 * n, phi_out + g, n, pi_out + g, 0, tj);
-                    }
+                    const bool do2 = p >= p0 && p < p1;
+                    const int s1 = (q - p0) & (L1_SLOTS - 1);
+                    round(do1 ? V1 : 0, ring + (size_t)ca.s * stage_n, ring + (size_t)cb.s * stage_n,
+                          ring + (size_t)cc.s * stage_n, l1 + (size_t)s1 * slot_n, do2 ? V2 : 0,
+                          l1 + (size_t)((s1 + 1) & (L1_SLOTS - 1)) * slot_n,
+                          l1 + (size_t)((s1 + 2) & (L1_SLOTS - 1)) * slot_n,
+                          l1 + (size_t)((s1 + 3) & (L1_SLOTS - 1)) * slot_n, ((size_t)p * n + j0) * n);
                 }
                 /* input plane q - 2 has had its last use (level 1 at plane q - 1);
                  * the round after the last input plane only runs level 2 */
@@ -310,7 +312,7 @@ __global__ void __launch_bounds__(TB_NT, 1)
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&empty[ca.s]);
                 }
-                if (tb_consumer_any(bad)) {
+                if (tb_consumer_any(bad, NC)) {
                     run = false;
                     break;
                 }
@@ -352,9 +354,9 @@ int sm_count();
 /* Geometry of the two-step pass: float fields, d = 3, static background,
  * n a multiple of 4 in [64, 1024]. TJ rows with TJ * n about 2048 sites (4
  * at 512^3, 8 at 256^3); shared memory = the input ring (4..6 stages) + the
- * 4 level-1 planes, one block per SM; the number of plane parts balances an
- * item's fixed cost (its 4 halo input planes, 2 extra level-1 planes) against
- * a part-filled last round. */
+ * 4 level-1 planes, one block per SM; the number of plane parts minimises
+ * whole rounds of items over the SMs times an item's planes (measured: 9
+ * parts at 256^3, 8 at 512^3). */
 bool step3tb_geometry(const StepConst &k, int prec, int tl, int &tj, int &nstage, size_t &smem, unsigned &grid,
                       int &parts) {
     if (k.d != 3 || prec != P_FP32 || k.expanding || tl != 2) return false;
@@ -373,13 +375,14 @@ bool step3tb_geometry(const StepConst &k, int prec, int tl, int &tj, int &nstage
     smem = TB_HDR + (size_t)nstage * stage + lev;
     const long long ntiles = n / tj;
     const long long slots = sm_count();
-    const double fixed = 3.0;
+    /* whole rounds of items over the SMs (one block each), an item costing
+     * its planes plus about one plane */
     double best = 1e300;
     parts = 1;
     for (int P = 1; P <= n / 4; ++P) {
-        const double per_item = (double)n / P + fixed;
-        const long long nitems = ntiles * P;
-        const double cost = nitems <= slots ? per_item : (double)nitems / slots * per_item + 0.5 * per_item;
+        const double per_item = (double)n / P + 1.0;
+        const long long rounds = (ntiles * P + slots - 1) / slots;
+        const double cost = (double)rounds * per_item;
         if (cost < best - 1e-9) {
             best = cost;
             parts = P;
@@ -392,6 +395,27 @@ bool step3tb_geometry(const StepConst &k, int prec, int tl, int &tj, int &nstage
     return true;
 }
 
+/* Consumer threads of the two-step pass: a multiple of 32 near (vectors of
+ * both levels per input plane) / k, k = 2 (or 1, 3, 4), so that every
+ * consumer thread has the same number of vectors in a round; at most 21
+ * consumer warps. */
+int step3tb_consumers(const StepConst &k, int tj) {
+    const int nvr = k.n / 4;
+    const int vt = (2 * tj + 2) * nvr;
+    int best = 0;
+    double best_waste = 1e300;
+    for (int per : {2, 3, 1, 4}) {
+        const int nc = ((vt + per - 1) / per + 31) / 32 * 32;
+        if (nc < 256 || nc > TB_MAXT - 32) continue;
+        const double waste = (double)(per * nc - vt) / vt;
+        if (waste < best_waste - 1e-9) {
+            best_waste = waste;
+            best = nc;
+        }
+    }
+    return best ? best : 512;
+}
+
 cudaError_t launch_step3_tb(int prec, const StepConst &k, int tl, const void *phi_in, const void *pi_in,
                             void *phi_out, void *pi_out, DevState *st, cudaStream_t s) {
     int tj, nstage, parts;
@@ -400,7 +424,8 @@ cudaError_t launch_step3_tb(int prec, const StepConst &k, int tl, const void *ph
     if (!step3tb_geometry(k, prec, tl, tj, nstage, smem, grid, parts)) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(k_step3_t2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_step3_t2<<<grid, TB_NT, smem, s>>>(k, tj, nstage, parts, (const float *)phi_in, (const float *)pi_in,
+    const int nc = step3tb_consumers(k, tj);
+    k_step3_t2<<<grid, nc + 32, smem, s>>>(k, tj, nstage, parts, (const float *)phi_in, (const float *)pi_in,
                                         (float *)phi_out, (float *)pi_out, st);
     return cudaGetLastError();
 }
