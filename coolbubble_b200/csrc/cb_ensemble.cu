@@ -32,10 +32,12 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "cb_handle.h"
 #include "cb_step_common.cuh"
+#include "cb_tma.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -93,6 +95,48 @@ __device__ __forceinline__ void vset<double>(double2 &v, int s, double x) {
     if (s == 0) v.x = x; else v.y = x;
 }
 
+/* Packed-pair constants of the float path of the d = 2 step (a = 1). */
+struct Pk2 {
+    F2 idx2, dt, nc2, c3, nc4;
+};
+
+/* One 16-byte vector of a d = 2 step without sums as two packed f32x2 pairs
+ * (float only; the double kernel never calls it): pi' = pi + dt F(phi),
+ * phi' = phi + dt pi' with F = lap / dx^2 - V'(phi) (bubble.cpp:716-743,
+ * 853-856, 867-870; a = 1), V'(f) = f (c2 + f (-c3 + f c4)) negated exactly by
+ * negating its coefficients. */
+template <typename T>
+struct Packed2D {
+    template <typename V, typename S>
+    static __device__ __forceinline__ void run(const V &, const V &, const V &, S, S, const V &, const Pk2 &, V &,
+                                               V &) {}
+};
+template <>
+struct Packed2D<float> {
+    static __device__ __forceinline__ void run(const float4 &c, const float4 &um, const float4 &up, float left,
+                                               float right, const float4 &pv, const Pk2 &K, float4 &phi_new,
+                                               float4 &pi_new) {
+        auto pair = [&](F2 cc, F2 umm, F2 upp, F2 kmm, F2 kpp, F2 pp, F2 &phi2, F2 &pi2) {
+            const F2 two = f2_add(cc, cc);
+            const F2 t0 = f2_add(f2_sub(upp, two), umm);
+            const F2 t1 = f2_add(f2_sub(kpp, two), kmm);
+            const F2 lap = f2_add(t0, t1);
+            const F2 nh = f2_fma(cc, f2_fma(cc, K.nc4, K.c3), K.nc2);
+            const F2 force = f2_fma(lap, K.idx2, f2_mul(cc, nh));
+            pi2 = f2_fma(K.dt, force, pp);
+            phi2 = f2_fma(K.dt, pi2, cc);
+        };
+        const F2 mid = f2_pack(c.y, c.z);
+        F2 phi01, pi01, phi23, pi23;
+        pair(f2_pack(c.x, c.y), f2_pack(um.x, um.y), f2_pack(up.x, up.y), f2_pack(left, c.x), mid, f2_pack(pv.x, pv.y),
+             phi01, pi01);
+        pair(f2_pack(c.z, c.w), f2_pack(um.z, um.w), f2_pack(up.z, up.w), mid, f2_pack(c.w, right), f2_pack(pv.z, pv.w),
+             phi23, pi23);
+        phi_new = make_float4(f2_lo(phi01), f2_hi(phi01), f2_lo(phi23), f2_hi(phi23));
+        pi_new = make_float4(f2_lo(pi01), f2_hi(pi01), f2_lo(pi23), f2_hi(pi23));
+    }
+};
+
 /* Resident d = 2 kernel: blockIdx.x / cs is the member, the cluster rank the slab. */
 template <typename T>
 __global__ void k_ensemble2d(const EnsMember *__restrict__ members, int cs, int nsteps, int sums_every,
@@ -137,6 +181,16 @@ __global__ void k_ensemble2d(const EnsMember *__restrict__ members, int cs, int 
     const int up_rank = (rank + 1) % cs, dn_rank = (rank - 1 + cs) % cs;
     const int nvr = n / W;
     const int nv = R * nvr;
+    /* this thread's first (row, vector) of the slab; later ones step by nt */
+    const int r_first = tid / nvr, kv_first = tid % nvr;
+    const int row_step = nt / nvr, vec_step = nt % nvr;
+    /* packed-pair constants of the float path (a = 1) */
+    Pk2 pk;
+    pk.idx2 = f2_splat(k.inv_dx2f);
+    pk.dt = f2_splat(k.dtf);
+    pk.nc2 = f2_splat(-k.c2f);
+    pk.c3 = f2_splat(k.c3f);
+    pk.nc4 = f2_splat(-k.c4f);
     int event = 0;
 
     for (int step = 0; step < nsteps; ++step) {
@@ -147,58 +201,73 @@ __global__ void k_ensemble2d(const EnsMember *__restrict__ members, int cs, int 
         const T *row_before = cluster.map_shared_rank(cur, dn_rank) + (size_t)(R - 1) * n;
         const bool sums = sums_every > 0 && ((step + 1) % sums_every == 0);
         Acc<T> acc[NSUM];
-        for (int v = tid; v < nv; v += nt) {
-            const int r = v / nvr;
-            const int kk = (v - r * nvr) * W;
-            const size_t o = (size_t)r * n + kk;
-            const VT c = *reinterpret_cast<const VT *>(cur + o);
-            const VT um = *reinterpret_cast<const VT *>(r > 0 ? cur + o - n : row_before + kk);
-            const VT up = *reinterpret_cast<const VT *>(r + 1 < R ? cur + o + n : row_after + kk);
-            const VT pv = *reinterpret_cast<const VT *>(pis + o);
-            const T left = cur[(size_t)r * n + (kk == 0 ? n - 1 : kk - 1)];
-            const T right = cur[(size_t)r * n + (kk + W == n ? 0 : kk + W)];
-            VT phi_new, pi_new;
-#pragma unroll
-            for (int s = 0; s < W; ++s) {
-                const T f = vget<T>(c, s);
-                const T kmn = s == 0 ? left : vget<T>(c, s - 1);
-                const T kpl = s == W - 1 ? right : vget<T>(c, s + 1);
-                const T two = A::add(f, f);
-                /* Laplacian, axis 0 (rows) then axis 1 (columns) (bubble.cpp:731-736); a = 1 */
-                const T t0 = A::add(A::sub(vget<T>(up, s), two), vget<T>(um, s));
-                const T t1 = A::add(A::sub(kpl, two), kmn);
-                const T lap = A::add(t0, t1);
-                const T force = A::sub(dx2_pow2 ? A::mul(lap, inv_dx2) : A::div(lap, dx2), dV<T>(k, f));
-                const T pold = vget<T>(pv, s);
-                const T pn = A::add(pold, A::mul(dt, force));
-                vset<T>(pi_new, s, pn);
-                vset<T>(phi_new, s, A::add(f, A::mul(dt, pn)));
-                if (sums) {
-                    /* forward gradients: x <- axis 1, y <- axis 0 (bubble.cpp:794-796), a = 1 */
-                    const T gx = dx_pow2 ? A::mul(A::sub(kpl, f), inv_dx) : A::div(A::sub(kpl, f), dx);
-                    const T gy = dx_pow2 ? A::mul(A::sub(vget<T>(up, s), f), inv_dx)
-                                         : A::div(A::sub(vget<T>(up, s), f), dx);
-                    const T eg = A::mul(half, A::add(A::sq(gx), A::sq(gy)));
-                    const T ep = Vpot<T>(k, f);
-                    const T ek = A::mul(A::mul(kin_w, pn), pn);
-                    const T et = A::add(A::add(ek, eg), ep);
-                    acc[S_EK].add(ek);
-                    acc[S_EP].add(ep);
-                    acc[S_EG].add(eg);
-                    acc[S_PHI].add(f);
-                    acc[S_V].add(pn);
-                    acc[Q_EK].add(A::sq(ek));
-                    acc[Q_EP].add(A::sq(ep));
-                    acc[Q_EG].add(A::sq(eg));
-                    acc[Q_ET].add(A::sq(et));
-                    acc[Q_PHI].add(A::sq(f));
-                    acc[Q_V].add(A::sq(pn));
-                    acc[S_EKIN_IN].add(A::mul(A::mul(kin_w, pold), pold));
+        /* one step over the slab; sums only at event steps (a compile-time
+         * choice per loop); float steps without sums in packed f32x2 pairs */
+        auto sweep = [&](auto with_sums) {
+            constexpr bool SU = decltype(with_sums)::value;
+            int r = r_first, kv = kv_first;
+            for (int v = tid; v < nv; v += nt, r += row_step, kv += vec_step) {
+                if (kv >= nvr) {
+                    kv -= nvr;
+                    ++r;
                 }
+                const int kk = kv * W;
+                const size_t o = (size_t)r * n + kk;
+                const VT c = *reinterpret_cast<const VT *>(cur + o);
+                const VT um = *reinterpret_cast<const VT *>(r > 0 ? cur + o - n : row_before + kk);
+                const VT up = *reinterpret_cast<const VT *>(r + 1 < R ? cur + o + n : row_after + kk);
+                const VT pv = *reinterpret_cast<const VT *>(pis + o);
+                const T left = cur[(size_t)r * n + (kk == 0 ? n - 1 : kk - 1)];
+                const T right = cur[(size_t)r * n + (kk + W == n ? 0 : kk + W)];
+                VT phi_new, pi_new;
+                if constexpr (!SU && std::is_same<T, float>::value) {
+                    Packed2D<T>::run(c, um, up, left, right, pv, pk, phi_new, pi_new);
+                } else {
+#pragma unroll
+                    for (int s = 0; s < W; ++s) {
+                        const T f = vget<T>(c, s);
+                        const T kmn = s == 0 ? left : vget<T>(c, s - 1);
+                        const T kpl = s == W - 1 ? right : vget<T>(c, s + 1);
+                        const T two = A::add(f, f);
+                        /* Laplacian, axis 0 (rows) then axis 1 (columns) (bubble.cpp:731-736); a = 1 */
+                        const T t0 = A::add(A::sub(vget<T>(up, s), two), vget<T>(um, s));
+                        const T t1 = A::add(A::sub(kpl, two), kmn);
+                        const T lap = A::add(t0, t1);
+                        const T force = A::sub(dx2_pow2 ? A::mul(lap, inv_dx2) : A::div(lap, dx2), dV<T>(k, f));
+                        const T pold = vget<T>(pv, s);
+                        const T pn = A::add(pold, A::mul(dt, force));
+                        vset<T>(pi_new, s, pn);
+                        vset<T>(phi_new, s, A::add(f, A::mul(dt, pn)));
+                        if constexpr (SU) {
+                            /* forward gradients: x <- axis 1, y <- axis 0 (bubble.cpp:794-796), a = 1 */
+                            const T gx = dx_pow2 ? A::mul(A::sub(kpl, f), inv_dx) : A::div(A::sub(kpl, f), dx);
+                            const T gy = dx_pow2 ? A::mul(A::sub(vget<T>(up, s), f), inv_dx)
+                                                 : A::div(A::sub(vget<T>(up, s), f), dx);
+                            const T eg = A::mul(half, A::add(A::sq(gx), A::sq(gy)));
+                            const T ep = Vpot<T>(k, f);
+                            const T ek = A::mul(A::mul(kin_w, pn), pn);
+                            const T et = A::add(A::add(ek, eg), ep);
+                            acc[S_EK].add(ek);
+                            acc[S_EP].add(ep);
+                            acc[S_EG].add(eg);
+                            acc[S_PHI].add(f);
+                            acc[S_V].add(pn);
+                            acc[Q_EK].add(A::sq(ek));
+                            acc[Q_EP].add(A::sq(ep));
+                            acc[Q_EG].add(A::sq(eg));
+                            acc[Q_ET].add(A::sq(et));
+                            acc[Q_PHI].add(A::sq(f));
+                            acc[Q_V].add(A::sq(pn));
+                            acc[S_EKIN_IN].add(A::mul(A::mul(kin_w, pold), pold));
+                        }
+                    }
+                }
+                *reinterpret_cast<VT *>(nxt + o) = phi_new;
+                *reinterpret_cast<VT *>(pis + o) = pi_new;
             }
-            *reinterpret_cast<VT *>(nxt + o) = phi_new;
-            *reinterpret_cast<VT *>(pis + o) = pi_new;
-        }
+        };
+        if (sums) sweep(std::true_type{});
+        else sweep(std::false_type{});
         if (sums) {
             /* per CTA: warps by shuffle, then warps in order (double) */
 #pragma unroll

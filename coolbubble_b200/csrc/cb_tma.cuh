@@ -115,16 +115,8 @@ __device__ __forceinline__ F2 f2_pack(float a, float b) {
     return r;
 }
 __device__ __forceinline__ F2 f2_splat(float a) { return f2_pack(a, a); }
-__device__ __forceinline__ float f2_lo(F2 x) {
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v));
-    return a;
-}
-__device__ __forceinline__ float f2_hi(F2 x) {
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v));
-    return b;
-}
+__device__ __forceinline__ float f2_lo(F2 x) { return __uint_as_float((unsigned)(x.v & 0xffffffffull)); }
+__device__ __forceinline__ float f2_hi(F2 x) { return __uint_as_float((unsigned)(x.v >> 32)); }
 __device__ __forceinline__ F2 f2_add(F2 a, F2 b) {
     F2 r;
     asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
