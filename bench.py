@@ -540,7 +540,8 @@ def main():
 
     peak, peak_kind = measured_peak()
     per_launch_ms = ms / launches
-    alg_bytes = BYTES_PER_SITE[prec] * N * args.steps / launches   # per launch: units (site-updates) x 16 B
+    # every launch (one step, or a two-step pass) reads phi and pi once and writes them once
+    alg_bytes = BYTES_PER_SITE[prec] * N
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
     line = {
         "metric": "lattice site-updates/s", "value": value, "unit": "site-updates/s", "n_gpus": ws,
@@ -550,9 +551,14 @@ def main():
                    "expansion": w["expansion"], "precision": prec, "parallelism": f"replicas{ws}",
                    "l2": "inputs larger than L2 (2 x 512^3 floats = 1 GiB)",
                    "sums_every": OUT_ENERGY_EVERY, "ic": "seeded gaussian fluctuations, amplitude 0.05",
-                   "steps_per_pass": int(os.environ.get("CB_TEMPORAL_BLOCK", "1")) if (prec == "fp32c" and not w["expansion"]) else 1},
+                   "steps_per_launch": args.steps / launches,
+                   "temporal_block": os.environ.get("CB_TEMPORAL_BLOCK", "autotuned")},
         "fp64_value": value64, "fp64_ms_per_step": ms64 / k64, "speedup_vs_fp64": value / value64,
         "hbm_gbs": achieved,
+        # site-updates/s x the 16 B a one-step pass moves per site-update: above the
+        # DRAM rate when two-step passes move those bytes once per two steps
+        "effective_gbs": value * BYTES_PER_SITE[prec] / 1e9 / ws,
+        "effective_frac": value * BYTES_PER_SITE[prec] / 1e9 / ws / peak,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": committed_traffic(args.workload, prec), "peak_source": peak_kind,
                      "alg_bytes_per_launch": alg_bytes, "launch_ms": per_launch_ms,

@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -126,12 +127,11 @@ StepConst make_const(const cb_params *p) {
     k.want_local = 0;
     const char *path = std::getenv("CB_STEP_PATH");
     k.force_generic = (path && std::string(path) == "generic") ? 1 : 0;
-    /* steps per pass of the temporally blocked static kernel (CB_TEMPORAL_BLOCK=2 or 3 turns
-     * it on; off by default: on B200 it does not yet beat the single-step pass, which runs at
-     * 0.95 of the copy bandwidth) */
+    /* steps per pass of the static float 3-D step: CB_TEMPORAL_BLOCK=1 or 2 fixes it;
+     * unset, it is chosen per lattice size by timing both passes once (0: not chosen yet) */
     const char *tb = std::getenv("CB_TEMPORAL_BLOCK");
-    k.temporal = tb ? std::atoi(tb) : 1;
-    if (k.temporal < 1 || k.force_generic) k.temporal = 1;
+    k.temporal = tb ? std::max(1, std::atoi(tb)) : 0;
+    if (k.force_generic) k.temporal = 1;
     return k;
 }
 
@@ -341,6 +341,60 @@ int ensure_tmp(cb_handle *h, size_t bytes) {
     return CB_OK;
 }
 
+/* The temporal-block autotuner: for a static float 3-D run whose lattice the
+ * two-step pass can take, time one-step and two-step passes on the run's own
+ * stream (each reads the current fields and writes the spare buffers, so the
+ * run's state does not change) and keep whichever moves a step faster; the
+ * choice is cached per device and lattice size. Both passes give the same
+ * fields bit for bit, so the choice only changes the speed. */
+int choose_temporal(cb_handle *h) {
+    if (h->expanding || h->prec != P_FP32 || h->p.d != 3) return 1;
+    int tj, ns, parts;
+    size_t sm;
+    unsigned g;
+    if (!step3tb_geometry(h->k, h->prec, 2, tj, ns, sm, g, parts)) return 1;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return 1; }
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, int> cache;
+    const std::pair<int, int> key(dev, h->p.n_grids);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    cudaEvent_t ev[3];
+    for (auto &x : ev)
+        if (cudaEventCreate(&x) != cudaSuccess) { cudaGetLastError(); return 1; }
+    const int i = h->cphi, j = h->cpi;
+    StepConst k = h->k;
+    k.want_local = 0;
+    auto one = [&]() {
+        return launch_step(h->prec, k, false, 0, h->phi[i], h->pi[j], h->phi[1 - i], h->pi[1 - j], h->loc[0],
+                           h->loc[1], h->loc[2], h->st, h->partials, h->stream);
+    };
+    auto two = [&]() { return launch_step3_tb(h->prec, k, 2, h->phi[i], h->pi[j], h->phi[1 - i], h->pi[1 - j], h->st, h->stream); };
+    const int reps = 4;
+    cudaError_t e = one();
+    if (e == cudaSuccess) e = two();
+    if (e == cudaSuccess) e = cudaEventRecord(ev[0], h->stream);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = one();
+    if (e == cudaSuccess) e = cudaEventRecord(ev[1], h->stream);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = two();
+    if (e == cudaSuccess) e = cudaEventRecord(ev[2], h->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev[2]);
+    float t1 = 0.f, t2 = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t1, ev[0], ev[1]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t2, ev[1], ev[2]);
+    for (auto &x : ev) cudaEventDestroy(x);
+    if (e != cudaSuccess) { cudaGetLastError(); return 1; }
+    /* per step: t1 / reps against t2 / (2 reps); keep the two-step pass only for a clear gain */
+    const int tl = (t2 / 2.f < 0.97f * t1) ? 2 : 1;
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = tl;
+    return tl;
+}
+
 int step_impl(cb_handle *h, int nsteps, int flags, bool timed) {
     if (nsteps < 0) return fail(h, CB_EINVAL, "nsteps must be non-negative");
     if ((flags & ~(CB_STEP_SUMS | CB_STEP_LOCAL)) != 0) return fail(h, CB_EINVAL, "unknown flag bits");
@@ -356,6 +410,7 @@ int step_impl(cb_handle *h, int nsteps, int flags, bool timed) {
     int tj, ns, cz;
     size_t sm;
     unsigned g;
+    if (h->k.temporal == 0 && nsteps > 2) h->k.temporal = choose_temporal(h);
     const int tl = h->k.temporal;
     const bool tb_ok = !h->expanding && tl > 1 && step3tb_geometry(h->k, h->prec, tl, tj, ns, sm, g, cz);
     for (int it = 1; it <= nsteps;) {

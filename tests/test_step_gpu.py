@@ -319,3 +319,26 @@ def test_line_equals_the_field(case):
     want = phi[idx] if d == 1 else (phi[idx, i1] if d == 2 else phi[idx, i1, i2])
     np.testing.assert_array_equal(line, want)
     np.testing.assert_array_equal(s.line(i0, i1, i2, count=7), want[:7])
+
+
+def test_temporal_block_autotuner_keeps_the_fields(monkeypatch):
+    """With CB_TEMPORAL_BLOCK unset the steps per pass of a static float 3-D
+    run are chosen by timing both passes once (on spare buffers: the run's
+    state does not change); the fields equal those of one-step passes bit for
+    bit whatever the choice."""
+    import coolbubble_b200 as cb
+    d, n, L, c, steps = 3, 256, 32.0, 2.0, 41
+    phi0, pi0 = smooth_noise(d, n, 0.3, seed=41), smooth_noise(d, n, 0.05, seed=42)
+    p = cb.make_params(d, n, L, c, 0.1 * L / n, precision="fp32c", memorysave=1)
+    monkeypatch.delenv("CB_TEMPORAL_BLOCK", raising=False)
+    auto = cb.Bubble(p, phi0, pi0)
+    monkeypatch.setenv("CB_TEMPORAL_BLOCK", "1")
+    single = cb.Bubble(p, phi0, pi0)
+    monkeypatch.delenv("CB_TEMPORAL_BLOCK")
+    a, b = auto.step(steps, sums=True), single.step(steps, sums=True)
+    launches, nsteps = auto.counters()
+    assert nsteps == steps and launches in (steps, steps // 2 + 1)   # one-step or two-step passes
+    assert a == b
+    fa, fb = auto.fields(local=False), single.fields(local=False)
+    for k in ("phi", "pi"):
+        np.testing.assert_array_equal(fa[k], fb[k])
