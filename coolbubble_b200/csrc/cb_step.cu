@@ -41,6 +41,7 @@
 #include <type_traits>
 
 #include "cb_internal.h"
+#include "cb_launch.cuh"
 #include "cb_step_common.cuh"
 
 namespace cb {
@@ -60,6 +61,8 @@ __global__ void __launch_bounds__(TX *TY) k_step(StepConst k, const T *__restric
                                                    double *partials) {
     using A = Ar<T>;
     __shared__ T tile[TY + 2][TX + 2];
+    pdl_wait();          /* the previous step's fields and device state */
+    pdl_allow_next();
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int ni = k.ni, nj = k.nj, nk = k.nk;
     const int kk = blockIdx.x * TX + tx;
@@ -382,14 +385,11 @@ template <typename T, int D, bool DF, int SUMS>
 cudaError_t launch_t(const StepConst &k, const void *phi_in, const void *pi_in, void *phi_out, void *pi_out,
                      void *le, void *lg, void *lp, DevState *st, double *partials, cudaStream_t s) {
     const dim3 g = step_grid(k);
-    if (D == 1) {
-        k_step<T, 1, TX1, TY1, DF, SUMS><<<g, dim3(TX1, TY1), 0, s>>>(
-            k, (const T *)phi_in, (const T *)pi_in, (T *)phi_out, (T *)pi_out, (T *)le, (T *)lg, (T *)lp, st, partials);
-    } else {
-        k_step<T, D, TX3, TY3, DF, SUMS><<<g, dim3(TX3, TY3), 0, s>>>(
-            k, (const T *)phi_in, (const T *)pi_in, (T *)phi_out, (T *)pi_out, (T *)le, (T *)lg, (T *)lp, st, partials);
-    }
-    return cudaGetLastError();
+    if (D == 1)
+        return launch_pdl(k_step<T, 1, TX1, TY1, DF, SUMS>, g, dim3(TX1, TY1), 0, s, k, (const T *)phi_in,
+                          (const T *)pi_in, (T *)phi_out, (T *)pi_out, (T *)le, (T *)lg, (T *)lp, st, partials);
+    return launch_pdl(k_step<T, D, TX3, TY3, DF, SUMS>, g, dim3(TX3, TY3), 0, s, k, (const T *)phi_in,
+                      (const T *)pi_in, (T *)phi_out, (T *)pi_out, (T *)le, (T *)lg, (T *)lp, st, partials);
 }
 
 template <typename T, int D>

@@ -33,6 +33,7 @@
 #include <type_traits>
 
 #include "cb_internal.h"
+#include "cb_launch.cuh"
 #include "cb_step_common.cuh"
 #include "cb_tma.cuh"
 
@@ -144,6 +145,8 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         fence_mbar_init();
     }
     __syncthreads();
+    pdl_wait();          /* the previous step's fields, device state and work queue */
+    pdl_allow_next();
 
     Acc<T> acc[NSUM];
 
@@ -662,8 +665,9 @@ cudaError_t launch_step3(int prec, const StepConst &k, bool df, int sums, const 
         auto fn = k_step3<T, DFv, SU>;                                                                             \
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);          \
         if (e != cudaSuccess) return e;                                                                            \
-        fn<<<grid, NT3, smem, s>>>(k, tj, nstage, parts, (const T *)phi_in, (const T *)pi_in, (T *)phi_out,        \
-                                   (T *)pi_out, (T *)le, (T *)lg, (T *)lp, st, partials);                          \
+        e = launch_pdl(fn, dim3(grid), dim3(NT3), smem, s, k, tj, nstage, parts, (const T *)phi_in,                \
+                       (const T *)pi_in, (T *)phi_out, (T *)pi_out, (T *)le, (T *)lg, (T *)lp, st, partials);     \
+        if (e != cudaSuccess) return e;                                                                            \
     } while (0)
     if (prec == P_FP64) {
         if (df && sums == SUM_FULL) CB_LAUNCH3(double, true, SUM_FULL);

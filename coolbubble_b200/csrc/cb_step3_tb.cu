@@ -34,6 +34,7 @@
 #include <cstdlib>
 
 #include "cb_internal.h"
+#include "cb_launch.cuh"
 #include "cb_step_common.cuh"
 #include "cb_tma.cuh"
 
@@ -156,6 +157,8 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
         fence_mbar_init();
     }
     __syncthreads();
+    pdl_wait();          /* the previous step's fields, device state and work queue */
+    pdl_allow_next();
 
     if (warp == CW) {
         /* ---- producer: each item's input planes p0 - 2 .. p1 + 1 ---- */
@@ -425,9 +428,8 @@ cudaError_t launch_step3_tb(int prec, const StepConst &k, int tl, const void *ph
     cudaError_t e = cudaFuncSetAttribute(k_step3_t2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int nc = step3tb_consumers(k, tj);
-    k_step3_t2<<<grid, nc + 32, smem, s>>>(k, tj, nstage, parts, (const float *)phi_in, (const float *)pi_in,
-                                        (float *)phi_out, (float *)pi_out, st);
-    return cudaGetLastError();
+    return launch_pdl(k_step3_t2, dim3(grid), dim3(nc + 32), smem, s, k, tj, nstage, parts, (const float *)phi_in,
+                      (const float *)pi_in, (float *)phi_out, (float *)pi_out, st);
 }
 
 }  // namespace cb
