@@ -47,6 +47,8 @@ CASES = {
     "d3_thermal": dict(d=3, n=16, L=32.0, c=2.0, mode=-3, steps=100, trad=0.05),
     "d3_odd_dx": dict(d=3, n=12, L=16.0, c=4.0, mode=1, steps=100, expansion=1, mpl=10.0, nbubbles=3),
     "d3_thermal_expanding": dict(d=3, n=12, L=24.0, c=3.0, mode=-3, steps=60, trad=0.1, expansion=1, mpl=10.0),
+    # conformal time (ALPHAVAL = 1): the gradient energy enters the Friedmann update
+    "d3_conformal": dict(d=3, n=16, L=16.0, c=4.0, mode=1, steps=100, expansion=1, mpl=10.0, nbubbles=4, alpha=1),
 }
 
 

@@ -131,6 +131,8 @@ def _oracle_run(d, n, L, c, dt, phi0, pi0, steps, every, **kw):
     dict(d=1, n=4096, L=64.0, c=4.0, steps=100, every=25, ic="noise"),
     # dx^2 not a power of two: the exact-division path
     dict(d=2, n=96, L=30.0, c=5.0, steps=80, every=20, ic="bubbles", nb=4),
+    # conformal time (ALPHAVAL = 1) on the staged d = 3 kernel: gradient energy in every Friedmann update
+    dict(d=3, n=64, L=16.0, c=4.0, steps=60, every=20, ic="bubbles", nb=6, expansion=1, mpl=10.0, alpha=1),
 ])
 def test_fp64_matches_oracle(case):
     import coolbubble_b200 as cb
@@ -141,7 +143,7 @@ def test_fp64_matches_oracle(case):
     else:
         phi0 = smooth_noise(d, n, 0.3, seed=3)
         pi0 = smooth_noise(d, n, 0.05, seed=4)
-    kw = dict(expansion=case.get("expansion", 0), mpl=case.get("mpl", 200.0))
+    kw = dict(expansion=case.get("expansion", 0), mpl=case.get("mpl", 200.0), alpha=case.get("alpha", 0))
     o, ref = _oracle_run(d, n, L, c, dt, phi0, pi0, case["steps"], case["every"], **kw)
     s = cb.Bubble(cb.make_params(d, n, L, c, dt, **kw), phi0, pi0)
     for r in ref:
@@ -156,6 +158,7 @@ def test_fp64_matches_oracle(case):
     dict(d=3, n=64, L=16.0, c=4.0, steps=100, ic="bubbles", nb=8, expansion=1, mpl=10.0),
     dict(d=3, n=128, L=32.0, c=2.0, steps=100, ic="noise"),
     dict(d=2, n=256, L=32.0, c=4.0, steps=200, ic="bubbles", nb=5),
+    dict(d=3, n=64, L=16.0, c=4.0, steps=100, ic="bubbles", nb=8, expansion=1, mpl=10.0, alpha=1),
 ])
 def test_fp32c_energies_within_1e5_of_fp64_oracle(case):
     import coolbubble_b200 as cb
@@ -165,7 +168,7 @@ def test_fp32c_energies_within_1e5_of_fp64_oracle(case):
         phi0, pi0 = bubbles(d, n, L, c, case["nb"], seed=11), None
     else:
         phi0, pi0 = smooth_noise(d, n, 0.3, seed=5), smooth_noise(d, n, 0.05, seed=6)
-    kw = dict(expansion=case.get("expansion", 0), mpl=case.get("mpl", 200.0))
+    kw = dict(expansion=case.get("expansion", 0), mpl=case.get("mpl", 200.0), alpha=case.get("alpha", 0))
     o, ref = _oracle_run(d, n, L, c, dt, phi0, pi0, case["steps"], case["steps"], **kw)
     s = cb.Bubble(cb.make_params(d, n, L, c, dt, precision="fp32c", **kw), phi0, pi0)
     got = s.step(case["steps"], sums=True)
