@@ -28,6 +28,7 @@
  */
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdlib>
 #include <type_traits>
@@ -570,21 +571,21 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
 
 /* SMs of the current device (148 on B200; the same figure without a device). */
 int sm_count() {
-    static int cached[64] = {0};
+    static std::atomic<int> cached[64];   /* zero-initialised (static storage) */
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
         cudaGetLastError();
         return 148;
     }
-    if (cached[dev] == 0) {
-        int v = 0;
+    int v = cached[dev].load(std::memory_order_relaxed);
+    if (v == 0) {
         if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
             cudaGetLastError();
             v = 148;
         }
-        cached[dev] = v;
+        cached[dev].store(v, std::memory_order_relaxed);
     }
-    return cached[dev];
+    return v;
 }
 
 /* The tiled path covers d = 3 with n a multiple of the vector width, n >= 64
