@@ -49,12 +49,28 @@ constexpr int MAX_RADIX = 13;
 
 struct Plan {
     int n, nstages;
+    int logn;        /* log2 n if n is a power of two, else -1 */
     int radix[32];
 };
 
+/* q = x / m, r = x % m, by shifts when m = 2^lg (lg >= 0) */
+__device__ __forceinline__ void divmod(int x, int m, int lg, int &q, int &r) {
+    if (lg >= 0) {
+        q = x >> lg;
+        r = x & (m - 1);
+    } else {
+        q = x / m;
+        r = x - q * m;
+    }
+}
+__host__ __device__ __forceinline__ int log2_exact(int m) {
+    int l = 0;
+    while ((1 << l) < m) ++l;
+    return (1 << l) == m ? l : -1;
+}
+
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
-                        __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)));
+    return make_double2(fma(a.x, b.x, -(a.y * b.y)), fma(a.x, b.y, a.y * b.x));
 }
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
@@ -108,38 +124,48 @@ __device__ void dft_generic(double2 (&v)[MAX_RADIX], int R, const double2 *__res
  *   v_r = src[j + r n/R] * w^(r (j mod Ns) / (Ns R)),  v = DFT_R(v),
  *   dst[(j / Ns) Ns R + (j mod Ns) + r Ns] = v_r. */
 template <int R>
-__device__ void stage(const double2 *src, double2 *dst, int n, int C, int Ns, const double2 *__restrict__ tw,
-                      int rgen) {
+__device__ void stage(const double2 *src, double2 *dst, int n, int C, int logC, int Ns, int logNs,
+                      const double2 *__restrict__ tw, int rgen) {
     const int RR = R ? R : rgen;
     const int nb = n / RR;
     const int tw_scale = n / (Ns * RR);
     for (int idx = threadIdx.x; idx < nb * C; idx += blockDim.x) {
-        const int c = idx % C, j = idx / C;
-        const int jm = j % Ns;
+        const int c = idx & (C - 1), j = idx >> logC;   /* C is a power of two */
+        int jd, jm;
+        divmod(j, Ns, logNs, jd, jm);
         double2 v[MAX_RADIX];
-        for (int r = 0; r < RR; ++r) {
+#pragma unroll
+        for (int r = 0; r < (R ? R : MAX_RADIX); ++r) {
+            if (r >= RR) break;
             double2 x = src[(j + r * nb) * C + c];
-            if (r && jm) x = cmul(x, __ldg(&tw[(r * jm * tw_scale) % n]));
+            /* r jm tw_scale < RR Ns n / (Ns RR) = n: no wrap of the table index */
+            if (r && jm) x = cmul(x, __ldg(&tw[r * jm * tw_scale]));
             v[r] = x;
         }
         if constexpr (R == 0) dft_generic(v, RR, tw, n);
         else dft_small<R>(v, tw, n);
-        const int base = (j / Ns) * Ns * RR + jm;
-        for (int r = 0; r < RR; ++r) dst[(base + r * Ns) * C + c] = v[r];
+        const int base = jd * Ns * RR + jm;
+#pragma unroll
+        for (int r = 0; r < (R ? R : MAX_RADIX); ++r) {
+            if (r >= RR) break;
+            dst[(base + r * Ns) * C + c] = v[r];
+        }
     }
 }
 
 /* All stages; returns the buffer holding the result (a or b). */
 __device__ double2 *fft_smem(double2 *a, double2 *b, const Plan &pl, int C, const double2 *__restrict__ tw) {
     int Ns = 1;
+    const int logC = log2_exact(C);
     for (int s = 0; s < pl.nstages; ++s) {
         const int R = pl.radix[s];
+        const int logNs = log2_exact(Ns);
         switch (R) {
-            case 4: stage<4>(a, b, pl.n, C, Ns, tw, 4); break;
-            case 2: stage<2>(a, b, pl.n, C, Ns, tw, 2); break;
-            case 3: stage<3>(a, b, pl.n, C, Ns, tw, 3); break;
-            case 5: stage<5>(a, b, pl.n, C, Ns, tw, 5); break;
-            default: stage<0>(a, b, pl.n, C, Ns, tw, R); break;
+            case 4: stage<4>(a, b, pl.n, C, logC, Ns, logNs, tw, 4); break;
+            case 2: stage<2>(a, b, pl.n, C, logC, Ns, logNs, tw, 2); break;
+            case 3: stage<3>(a, b, pl.n, C, logC, Ns, logNs, tw, 3); break;
+            case 5: stage<5>(a, b, pl.n, C, logC, Ns, logNs, tw, 5); break;
+            default: stage<0>(a, b, pl.n, C, logC, Ns, logNs, tw, R); break;
         }
         __syncthreads();
         double2 *t = a; a = b; b = t;
@@ -157,7 +183,8 @@ __global__ void __launch_bounds__(FFT_T) k_fft_rows(Plan pl, const T *__restrict
     double2 *a = sm, *b = sm + (size_t)n * C;
     const size_t p0 = (size_t)blockIdx.x * C;
     for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
-        const int c = idx / n, i = idx % n;
+        int c, i;
+        divmod(idx, n, pl.logn, c, i);
         const size_t ra = 2 * (p0 + c), rb = ra + 1;
         double xa = 0.0, xb = 0.0;
         if (ra < rows) xa = (double)field[ra * n + i];
@@ -167,10 +194,10 @@ __global__ void __launch_bounds__(FFT_T) k_fft_rows(Plan pl, const T *__restrict
     __syncthreads();
     const double2 *z = fft_smem(a, b, pl, C, tw);
     for (int idx = threadIdx.x; idx < h * C; idx += blockDim.x) {
-        const int c = idx / h, k = idx % h;
+        const int c = idx / h, k = idx - (idx / h) * h;
         const size_t ra = 2 * (p0 + c), rb = ra + 1;
         const double2 zk = z[k * C + c];
-        const double2 zc = z[((n - k) % n) * C + c];
+        const double2 zc = z[(k == 0 ? 0 : n - k) * C + c];
         /* A = (Z_k + conj Z_{n-k}) / 2, B = (Z_k - conj Z_{n-k}) / (2i) */
         if (ra < rows) out[ra * h + k] = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y - zc.y));
         if (rb < rows) out[rb * h + k] = make_double2(0.5 * (zk.y + zc.y), -0.5 * (zk.x - zc.x));
@@ -188,8 +215,9 @@ __global__ void __launch_bounds__(FFT_T) k_fft_cols(Plan pl, double2 *data, size
     const size_t o = blockIdx.x / tiles_per_outer;
     const size_t q0 = (blockIdx.x % tiles_per_outer) * C;
     double2 *base = data + o * (size_t)n * inner;
+    const int logC = log2_exact(C);
     for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
-        const int c = idx % C, i = idx / C;
+        const int c = idx & (C - 1), i = idx >> logC;
         const size_t q = q0 + c;
         double2 x = q < inner ? base[(size_t)i * inner + q] : make_double2(0.0, 0.0);
         if (inverse) x.y = -x.y;   /* inverse DFT = conj(DFT(conj(x))) */
@@ -198,7 +226,7 @@ __global__ void __launch_bounds__(FFT_T) k_fft_cols(Plan pl, double2 *data, size
     __syncthreads();
     const double2 *z = fft_smem(a, b, pl, C, tw);
     for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
-        const int c = idx % C, i = idx / C;
+        const int c = idx & (C - 1), i = idx >> logC;
         const size_t q = q0 + c;
         double2 x = z[i * C + c];
         if (inverse) x.y = -x.y;
@@ -217,7 +245,8 @@ __global__ void __launch_bounds__(FFT_T) k_fft_rows_c2r(Plan pl, const double2 *
     double2 *a = sm, *b = sm + (size_t)n * C;
     const size_t p0 = (size_t)blockIdx.x * C;
     for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
-        const int c = idx / n, k = idx % n;
+        int c, k;
+        divmod(idx, n, pl.logn, c, k);
         const size_t ra = 2 * (p0 + c), rb = ra + 1;
         const bool mirror = k >= h;
         const int kk = mirror ? n - k : k;
@@ -232,7 +261,8 @@ __global__ void __launch_bounds__(FFT_T) k_fft_rows_c2r(Plan pl, const double2 *
     __syncthreads();
     const double2 *z = fft_smem(a, b, pl, C, tw);
     for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
-        const int c = idx / n, i = idx % n;
+        int c, i;
+        divmod(idx, n, pl.logn, c, i);
         const size_t ra = 2 * (p0 + c), rb = ra + 1;
         const double2 w = z[i * C + c];
         if (ra < rows) out[ra * n + i] = w.x;
@@ -249,42 +279,65 @@ struct BinConst {
 __device__ __forceinline__ long long sidx(long long i, int n) { return (i <= n / 2) ? i : i - n; }
 
 /* Shell sums of bubble.cpp:680-701 per block: smem histograms, then one row
- * of partials per block. */
+ * of partials per block. A warp takes a row of the half-complex array; each
+ * lane a contiguous run of the row's columns, along which the shell index
+ * only grows: the lane adds into registers while its shell stays the same and
+ * into the shared histogram when it changes. */
 __global__ void __launch_bounds__(FFT_T) k_bins(BinConst bc, const double2 *__restrict__ half, double *hist) {
     extern __shared__ double sh[];
     double *pw = sh, *ws = sh + bc.nbins, *ks = sh + 2 * bc.nbins;
     for (int i = threadIdx.x; i < 3 * bc.nbins; i += blockDim.x) sh[i] = 0.0;
     __syncthreads();
-    const size_t total = bc.rows * (size_t)bc.h;
-    for (size_t m = blockIdx.x * (size_t)blockDim.x + threadIdx.x; m < total; m += (size_t)gridDim.x * blockDim.x) {
-        const size_t r = m / bc.h;
-        const int j = (int)(m % bc.h);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int seg = (bc.h + 31) / 32;
+    const int j0 = lane * seg, j1 = min(bc.h, j0 + seg);
+    const unsigned rows = (unsigned)bc.rows;
+    for (unsigned r = blockIdx.x * nwarps + warp; r < rows; r += gridDim.x * nwarps) {
         double n2rows = 0.0;
         if (bc.d == 2) {
             const double s = (double)sidx((long long)r, bc.n);
             n2rows = s * s;
         } else if (bc.d == 3) {
-            const double s0 = (double)sidx((long long)(r / bc.n), bc.n), s1 = (double)sidx((long long)(r % bc.n), bc.n);
+            const unsigned q = r / (unsigned)bc.n, m = r - q * (unsigned)bc.n;
+            const double s0 = (double)sidx((long long)q, bc.n), s1 = (double)sidx((long long)m, bc.n);
             n2rows = __dadd_rn(s0 * s0, s1 * s1);
         }
-        const double nn = sqrt(__dadd_rn(n2rows, (double)j * (double)j));
-        const int b = (int)nn;
-        if (b >= bc.nbins) continue;
-        const double w = (j == 0 || j == bc.n / 2) ? 1.0 : 2.0;
-        const double2 f = half[m];
-        const double kc = __dmul_rn(nn, bc.dk);
-        double kd = kc;
-        if (bc.d >= 2) kd = __dmul_rn(kd, kc);
-        if (bc.d == 3) kd = __dmul_rn(kd, kc);
-        const double mag = __dadd_rn(__dmul_rn(f.x, f.x), __dmul_rn(f.y, f.y));
-        const double contrib = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(w, bc.pref), kd), bc.pnorm), mag);
-        atomicAdd(&pw[b], contrib);
-        atomicAdd(&ws[b], w);
-        atomicAdd(&ks[b], __dmul_rn(w, kc));
+        const double2 *row = half + (size_t)r * bc.h;
+        int cur = -1;
+        double ap = 0.0, aw = 0.0, ak = 0.0;
+        for (int j = j0; j < j1; ++j) {
+            const double nn = sqrt(__dadd_rn(n2rows, (double)j * (double)j));
+            const int b = (int)nn;
+            if (b >= bc.nbins) break;          /* the shell index grows with j */
+            if (b != cur) {
+                if (cur >= 0) {
+                    atomicAdd(&pw[cur], ap);
+                    atomicAdd(&ws[cur], aw);
+                    atomicAdd(&ks[cur], ak);
+                }
+                cur = b;
+                ap = aw = ak = 0.0;
+            }
+            const double w = (j == 0 || j == bc.n / 2) ? 1.0 : 2.0;
+            const double2 f = row[j];
+            const double kc = __dmul_rn(nn, bc.dk);
+            double kd = kc;
+            if (bc.d >= 2) kd = __dmul_rn(kd, kc);
+            if (bc.d == 3) kd = __dmul_rn(kd, kc);
+            const double mag = __dadd_rn(__dmul_rn(f.x, f.x), __dmul_rn(f.y, f.y));
+            ap = __dadd_rn(ap, __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(w, bc.pref), kd), bc.pnorm), mag));
+            aw = __dadd_rn(aw, w);
+            ak = __dadd_rn(ak, __dmul_rn(w, kc));
+        }
+        if (cur >= 0) {
+            atomicAdd(&pw[cur], ap);
+            atomicAdd(&ws[cur], aw);
+            atomicAdd(&ks[cur], ak);
+        }
     }
     __syncthreads();
-    double *row = hist + (size_t)blockIdx.x * 3 * bc.nbins;
-    for (int i = threadIdx.x; i < 3 * bc.nbins; i += blockDim.x) row[i] = sh[i];
+    double *out = hist + (size_t)blockIdx.x * 3 * bc.nbins;
+    for (int i = threadIdx.x; i < 3 * bc.nbins; i += blockDim.x) out[i] = sh[i];
 }
 
 /* Fixed-order sum of the per-block histograms. */
@@ -299,15 +352,16 @@ __global__ void k_bins_reduce(const double *__restrict__ hist, int nblk, int wid
 Plan plan_of(const FftState &f) {
     Plan p;
     p.n = f.n;
+    p.logn = log2_exact(f.n);
     p.nstages = f.nstages;
     for (int i = 0; i < 32; ++i) p.radix[i] = f.radix[i];
     return p;
 }
 
+/* columns per tile: a power of two (indices by shift), n C <= MAX_TILE_ELEMS, at most 16 */
 int tile_cols(int n) {
-    int C = MAX_TILE_ELEMS / n;
-    if (C < 1) C = 1;
-    if (C > 16) C = 16;
+    int C = 1;
+    while (C < 16 && 2 * C * n <= MAX_TILE_ELEMS) C *= 2;
     return C;
 }
 

@@ -18,7 +18,7 @@ def _ic_for(name):
     g = load_golden(name)
     m = g["meta"]
     p = cb.make_params(m["d"], m["n"], m["L"], m["c"], m["dt"], expansion=m.get("expansion", 0),
-                       mpl=m.get("mpl", 200.0))
+                       mpl=m.get("mpl", 200.0), alpha=m.get("alpha", 0))
     xns = g["xns"] if m["mode"] == 0 else None
     phi0, pi0, text = initial_condition(p, mode=m["mode"], n_bubbles=m.get("nbubbles", 5), trad=m.get("trad", 0.2),
                                         test=m.get("test", 0), xns=xns)

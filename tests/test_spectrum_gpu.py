@@ -51,7 +51,7 @@ def test_spectrum_matches_reference_golden(name):
     g = load_golden(name)
     m = g["meta"]
     p = cb.make_params(m["d"], m["n"], m["L"], m["c"], m["dt"], expansion=m.get("expansion", 0),
-                       mpl=m.get("mpl", 200.0))
+                       mpl=m.get("mpl", 200.0), alpha=m.get("alpha", 0))
     s = cb.Bubble(p, g["phi0"], g["pi0"])
     check_rows(s.ComputePowerSpectrum(), g["spec_start"])
     s.step(m["steps"], sums=True)
