@@ -5,7 +5,7 @@
  * FFTW's layout (unnormalised, row-major, last axis cut to n/2+1) followed
  * by shell binning of |phi_k|^2 with the d-dependent prefactor.
  *
- * DFT: a mixed-radix Stockham autosort FFT (radix 4, 2, 3, 5, and any other
+ * DFT: a mixed-radix Stockham autosort FFT (radix 8, 4, 2, 3, 5, and any other
  * small prime by a direct DFT of that size) held in shared memory, with
  * twiddles from a table computed once per length on the host in long
  * double. Three kinds of launches:
@@ -43,7 +43,7 @@ struct FftState {
 namespace {
 
 constexpr int FFT_T = 256;            /* threads per FFT block */
-constexpr int MAX_TILE_ELEMS = 4096;  /* n * C complex per buffer: 64 KiB, two buffers */
+constexpr int MAX_TILE_ELEMS = 2048;  /* n * C complex per buffer: 32 KiB, two buffers (3 blocks per SM) */
 constexpr int MAX_FFT_N = 6144;       /* n with C = 1: 2 * 6144 * 16 B = 192 KiB of shared memory */
 constexpr int MAX_RADIX = 13;
 
@@ -91,6 +91,34 @@ __device__ __forceinline__ void dft_small(double2 (&v)[MAX_RADIX], const double2
         v[2] = csub(a0, b0);
         v[1] = cadd(a1, mb1);
         v[3] = csub(a1, mb1);
+    } else if constexpr (R == 8) {
+        /* two DFTs of size 4 (even and odd inputs), then X_k = E_k + w^k O_k,
+         * X_{k+4} = E_k - w^k O_k with w = exp(-i pi / 4) */
+        auto dft4 = [](double2 &x0, double2 &x1, double2 &x2, double2 &x3) {
+            const double2 a0 = cadd(x0, x2), a1 = csub(x0, x2);
+            const double2 b0 = cadd(x1, x3), b1 = csub(x1, x3);
+            const double2 mb1 = make_double2(b1.y, -b1.x);
+            x0 = cadd(a0, b0);
+            x2 = csub(a0, b0);
+            x1 = cadd(a1, mb1);
+            x3 = csub(a1, mb1);
+        };
+        double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+        double2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+        dft4(e0, e1, e2, e3);
+        dft4(o0, o1, o2, o3);
+        const double h = 0.70710678118654752440;   /* sqrt(2) / 2 */
+        o1 = make_double2(h * (o1.x + o1.y), h * (o1.y - o1.x));
+        o2 = make_double2(o2.y, -o2.x);
+        o3 = make_double2(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+        v[0] = cadd(e0, o0);
+        v[4] = csub(e0, o0);
+        v[1] = cadd(e1, o1);
+        v[5] = csub(e1, o1);
+        v[2] = cadd(e2, o2);
+        v[6] = csub(e2, o2);
+        v[3] = cadd(e3, o3);
+        v[7] = csub(e3, o3);
     } else {
         /* direct DFT of size R with the table's roots: W_R^m = w_n^(m n / R) */
         double2 out[MAX_RADIX];
@@ -161,6 +189,7 @@ __device__ double2 *fft_smem(double2 *a, double2 *b, const Plan &pl, int C, cons
         const int R = pl.radix[s];
         const int logNs = log2_exact(Ns);
         switch (R) {
+            case 8: stage<8>(a, b, pl.n, C, logC, Ns, logNs, tw, 8); break;
             case 4: stage<4>(a, b, pl.n, C, logC, Ns, logNs, tw, 4); break;
             case 2: stage<2>(a, b, pl.n, C, logC, Ns, logNs, tw, 2); break;
             case 3: stage<3>(a, b, pl.n, C, logC, Ns, logNs, tw, 3); break;
@@ -304,11 +333,23 @@ __global__ void __launch_bounds__(FFT_T) k_bins(BinConst bc, const double2 *__re
         }
         const double2 *row = half + (size_t)r * bc.h;
         int cur = -1;
+        bool past = false;   /* beyond the last shell: so are the rest of the row's columns */
         double ap = 0.0, aw = 0.0, ak = 0.0;
-        for (int j = j0; j < j1; ++j) {
+        for (int jc = j0; jc < j1; jc += 8) {
+            /* the lane's next 8 values, loaded before any is used */
+            double2 fv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) fv[u] = jc + u < j1 ? __ldg(&row[jc + u]) : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+            const int j = jc + u;
+            if (j >= j1) break;
             const double nn = sqrt(__dadd_rn(n2rows, (double)j * (double)j));
             const int b = (int)nn;
-            if (b >= bc.nbins) break;          /* the shell index grows with j */
+            if (b >= bc.nbins) {               /* the shell index grows with j */
+                past = true;
+                break;
+            }
             if (b != cur) {
                 if (cur >= 0) {
                     atomicAdd(&pw[cur], ap);
@@ -319,7 +360,7 @@ __global__ void __launch_bounds__(FFT_T) k_bins(BinConst bc, const double2 *__re
                 ap = aw = ak = 0.0;
             }
             const double w = (j == 0 || j == bc.n / 2) ? 1.0 : 2.0;
-            const double2 f = row[j];
+            const double2 f = fv[u];
             const double kc = __dmul_rn(nn, bc.dk);
             double kd = kc;
             if (bc.d >= 2) kd = __dmul_rn(kd, kc);
@@ -328,6 +369,8 @@ __global__ void __launch_bounds__(FFT_T) k_bins(BinConst bc, const double2 *__re
             ap = __dadd_rn(ap, __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(w, bc.pref), kd), bc.pnorm), mag));
             aw = __dadd_rn(aw, w);
             ak = __dadd_rn(ak, __dmul_rn(w, kc));
+            }
+            if (past) break;
         }
         if (cur >= 0) {
             atomicAdd(&pw[cur], ap);
@@ -367,10 +410,11 @@ int tile_cols(int n) {
 
 size_t smem_bytes(int n, int C) { return 2 * (size_t)n * C * sizeof(double2); }
 
-/* Factor n into radices (4s first, then 2, 3, 5, other primes). */
+/* Factor n into radices (8s first, then 4, 2, 3, 5, other primes). */
 bool factor(int n, int *radix, int &ns) {
     ns = 0;
     int m = n;
+    while (m % 8 == 0) { radix[ns++] = 8; m /= 8; }
     while (m % 4 == 0) { radix[ns++] = 4; m /= 4; }
     while (m % 2 == 0) { radix[ns++] = 2; m /= 2; }
     for (int p = 3; p <= m && ns < 32; p += 2) {
@@ -419,7 +463,7 @@ int fft_setup(cb_handle *h, FftState *&out, int d, int n, cudaStream_t s) {
     for (int i = 0; i < d - 1; ++i) rows *= (size_t)n;
     f->half_elems = rows * hh;
     f->nbins = (int)(std::sqrt(double(d)) * n / 2) + 1;
-    f->hist_blocks = 148 * 2;
+    f->hist_blocks = 148 * 4;
     std::vector<double2> w = twiddles(n);
     cudaError_t e = cudaMallocAsync(&f->tw, n * sizeof(double2), s);
     if (e == cudaSuccess) e = cudaMallocAsync(&f->half, f->half_elems * sizeof(double2), s);
