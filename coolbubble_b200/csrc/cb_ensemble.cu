@@ -447,7 +447,7 @@ int autotune(cb_ensemble::Class &c, cb_handle *h0) {
     void *sphi = nullptr, *spi = nullptr;
     EnsMember *dm = nullptr;
     EnsRecord *drec = nullptr;
-    int best = 512;
+    int best = 256;
     float best_ms = 1e30f;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
@@ -465,9 +465,15 @@ int autotune(cb_ensemble::Class &c, cb_handle *h0) {
              cudaMemcpyAsync(spi, h0->pi[h0->cpi], bytes, cudaMemcpyDeviceToDevice, c.stream) == cudaSuccess &&
              cudaMemcpyAsync(dm, &m, sizeof m, cudaMemcpyHostToDevice, c.stream) == cudaSuccess;
     }
+    /* only block sizes the kernel's register use allows */
+    cudaFuncAttributes fa{};
+    cudaError_t ae = c.prec == P_FP64 ? cudaFuncGetAttributes(&fa, k_ensemble2d<double>)
+                                      : cudaFuncGetAttributes(&fa, k_ensemble2d<float>);
+    if (ae != cudaSuccess) { cudaGetLastError(); fa.maxThreadsPerBlock = 256; }
     const int cands[3] = {256, 512, 1024};
     for (int t : cands) {
         if (!ok) break;
+        if (t > fa.maxThreadsPerBlock) continue;
         if (launch_resident(c.prec, dm, 1, c.cs, t, 2, 0, drec, smem, c.stream) != cudaSuccess) { cudaGetLastError(); continue; }
         cudaEventRecord(a, c.stream);
         launch_resident(c.prec, dm, 1, c.cs, t, 40, 20, drec, smem, c.stream);
