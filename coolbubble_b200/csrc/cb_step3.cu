@@ -602,7 +602,9 @@ bool step3_geometry_parts(const StepConst &k, int prec, int &tj, int &nstage, si
     const int esz = prec == P_FP64 ? 8 : 4;
     const int W = 16 / esz;
     if (n % W != 0 || n < 64 || n > 1024) return false;
-    const int tile_sites = prec == P_FP64 ? 1024 : 2048;
+    int tile_sites = prec == P_FP64 ? 1024 : 2048;
+    const char *tenv = std::getenv("CB_STEP3_TILE");
+    if (tenv && std::atoi(tenv) >= 64) tile_sites = std::atoi(tenv);
     tj = 1;
     for (int t = 1; t <= n && t * n <= tile_sites; ++t)
         if (n % t == 0) tj = t;
@@ -610,7 +612,7 @@ bool step3_geometry_parts(const StepConst &k, int prec, int &tj, int &nstage, si
     const size_t stage = ((size_t)(tj + 2) + (size_t)(tj + (df ? 2 : 0))) * n * esz;
     const size_t budget = 106 * 1024;   /* two blocks per SM, with their static shared memory */
     nstage = (int)((budget - HDR) / stage);
-    if (nstage > 6) nstage = 6;
+    if (nstage > 8) nstage = 8;
     if (nstage < 4) nstage = 4;
     smem = HDR + nstage * stage;
     if (smem > 220 * 1024) return false;
