@@ -407,12 +407,12 @@ int step_impl(cb_handle *h, int nsteps, int flags, bool timed) {
     }
     /* steps that need nothing reported can run in temporally blocked passes */
     const bool want_last = (flags & (CB_STEP_SUMS | CB_STEP_LOCAL)) != 0;
-    int tj, ns, cz;
+    int tj, ns, parts;
     size_t sm;
     unsigned g;
     if (h->k.temporal == 0 && nsteps > 2) h->k.temporal = choose_temporal(h);
     const int tl = h->k.temporal;
-    const bool tb_ok = !h->expanding && tl > 1 && step3tb_geometry(h->k, h->prec, tl, tj, ns, sm, g, cz);
+    const bool tb_ok = !h->expanding && tl > 1 && step3tb_geometry(h->k, h->prec, tl, tj, ns, sm, g, parts);
     for (int it = 1; it <= nsteps;) {
         const int plain_left = nsteps - it + 1 - (want_last ? 1 : 0);
         if (tb_ok && plain_left >= tl) {

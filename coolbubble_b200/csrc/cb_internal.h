@@ -61,7 +61,7 @@ struct DevState {
 struct StepConst {
     int d, n;
     int ni, nj, nk;     /* extents mapped onto (march axis, tile rows, tile columns) */
-    int cz;             /* planes per block along the march axis (d = 3) */
+    int cz;             /* planes per block along the march axis (generic d = 3 kernel) */
     double dt;
     double c2, c3, c4;  /* V'(f) = c2 f - c3 f^2 + c4 f^3, coefficients as bubble.cpp:76 forms them */
     double v2, v3, v4, dv; /* V(f) = v2 f^2 - v3 f^3 + v4 f^4 + DeltaV (bubble.cpp:71) */
@@ -97,7 +97,7 @@ cudaError_t launch_step3(int prec, const StepConst &k, bool drift_first, int sum
 
 /* TL steps per pass, static float 3-D lattices (cb_step3_tb.cu). */
 bool step3tb_geometry(const StepConst &k, int prec, int tl, int &tj, int &nstage, size_t &smem, unsigned &grid,
-                      int &cz);
+                      int &parts);
 cudaError_t launch_step3_tb(int prec, const StepConst &k, int tl, const void *phi_in, const void *pi_in,
                             void *phi_out, void *pi_out, DevState *st, cudaStream_t s);
 
