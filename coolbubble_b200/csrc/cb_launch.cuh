@@ -1,13 +1,15 @@
 /* cb_launch.cuh -- programmatic dependent launch for the step kernels.
  *
  * Consecutive steps of a run are consecutive kernels on the run's stream. A
- * step kernel is launched with programmatic stream serialisation: it may be
- * scheduled while the previous step is still finishing (its blocks take the
- * slots the previous step's blocks leave) and it waits, in hardware, for the
- * previous grid to complete and its memory to be visible (griddepcontrol.wait)
- * before it reads anything that grid wrote. The launch latency of a step so
- * overlaps the tail of the one before. Without the launch attribute both
- * instructions do nothing.
+ * step kernel is launched with programmatic stream serialisation: once every
+ * block of the previous step has finished its sites (and said so with
+ * griddepcontrol.launch_dependents), the next step may be scheduled -- its
+ * blocks take the slots the finished blocks leave -- and it waits, in
+ * hardware, for the previous grid to complete and its memory to be visible
+ * (griddepcontrol.wait) before it reads anything that grid wrote. The launch
+ * latency of a step so overlaps the tail of the one before, and waiting blocks
+ * never hold slots that other streams' kernels could use for long. Without
+ * the launch attribute both instructions do nothing.
  */
 #ifndef CB_LAUNCH_CUH
 #define CB_LAUNCH_CUH

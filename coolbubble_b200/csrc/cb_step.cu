@@ -62,7 +62,6 @@ __global__ void __launch_bounds__(TX *TY) k_step(StepConst k, const T *__restric
     using A = Ar<T>;
     __shared__ T tile[TY + 2][TX + 2];
     pdl_wait();          /* the previous step's fields and device state */
-    pdl_allow_next();
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int ni = k.ni, nj = k.nj, nk = k.nk;
     const int kk = blockIdx.x * TX + tx;
@@ -178,6 +177,9 @@ __global__ void __launch_bounds__(TX *TY) k_step(StepConst k, const T *__restric
             pic = pinext;
         }
     }
+    /* this block's sites are done: the next step may be scheduled (its blocks
+     * take the slots the finished blocks leave) */
+    pdl_allow_next();
 
     if (SUMS != SUM_NONE) {
         double v[NSUM];

@@ -147,7 +147,6 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
     }
     __syncthreads();
     pdl_wait();          /* the previous step's fields, device state and work queue */
-    pdl_allow_next();
 
     Acc<T> acc[NSUM];
 
@@ -538,6 +537,9 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         }
     }
     __syncthreads();
+    /* this block's items are done: the next step may be scheduled (its blocks
+     * take the slots the finished blocks leave, and wait for this grid) */
+    pdl_allow_next();
     /* the last block out resets the work queue for the next launch on the stream */
     if (threadIdx.x == 0) {
         __threadfence();

@@ -158,7 +158,6 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
     }
     __syncthreads();
     pdl_wait();          /* the previous step's fields, device state and work queue */
-    pdl_allow_next();
 
     if (warp == CW) {
         /* ---- producer: each item's input planes p0 - 2 .. p1 + 1 ---- */
@@ -332,6 +331,8 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
         }
     }
     __syncthreads();
+    /* this block's items are done: the next step may be scheduled */
+    pdl_allow_next();
     if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(&st->item_done, 1u) == gridDim.x - 1) {
