@@ -211,14 +211,31 @@ __global__ void __launch_bounds__(FFT_T) k_fft_rows(Plan pl, const T *__restrict
     const int n = pl.n, h = n / 2 + 1;
     double2 *a = sm, *b = sm + (size_t)n * C;
     const size_t p0 = (size_t)blockIdx.x * C;
-    for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
-        int c, i;
-        divmod(idx, n, pl.logn, c, i);
-        const size_t ra = 2 * (p0 + c), rb = ra + 1;
-        double xa = 0.0, xb = 0.0;
-        if (ra < rows) xa = (double)field[ra * n + i];
-        if (rb < rows) xb = (double)field[rb * n + i];
-        a[i * C + c] = make_double2(xa, xb);
+    /* loads in batches of LB per thread, all issued before the first store */
+    constexpr int LB = 8;
+    for (int base = threadIdx.x; base < n * C; base += LB * blockDim.x) {
+        T xa[LB], xb[LB];
+#pragma unroll
+        for (int u = 0; u < LB; ++u) {
+            const int idx = base + u * blockDim.x;
+            xa[u] = xb[u] = (T)0;
+            if (idx < n * C) {
+                int c, i;
+                divmod(idx, n, pl.logn, c, i);
+                const size_t ra = 2 * (p0 + c), rb = ra + 1;
+                if (ra < rows) xa[u] = __ldg(&field[ra * n + i]);
+                if (rb < rows) xb[u] = __ldg(&field[rb * n + i]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < LB; ++u) {
+            const int idx = base + u * blockDim.x;
+            if (idx < n * C) {
+                int c, i;
+                divmod(idx, n, pl.logn, c, i);
+                a[i * C + c] = make_double2((double)xa[u], (double)xb[u]);
+            }
+        }
     }
     __syncthreads();
     const double2 *z = fft_smem(a, b, pl, C, tw);
@@ -245,12 +262,29 @@ __global__ void __launch_bounds__(FFT_T) k_fft_cols(Plan pl, double2 *data, size
     const size_t q0 = (blockIdx.x % tiles_per_outer) * C;
     double2 *base = data + o * (size_t)n * inner;
     const int logC = log2_exact(C);
-    for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
-        const int c = idx & (C - 1), i = idx >> logC;
-        const size_t q = q0 + c;
-        double2 x = q < inner ? base[(size_t)i * inner + q] : make_double2(0.0, 0.0);
-        if (inverse) x.y = -x.y;   /* inverse DFT = conj(DFT(conj(x))) */
-        a[i * C + c] = x;
+    /* loads in batches of LB per thread, all issued before the first store */
+    constexpr int LB = 8;
+    for (int b0 = threadIdx.x; b0 < n * C; b0 += LB * blockDim.x) {
+        double2 xs[LB];
+#pragma unroll
+        for (int u = 0; u < LB; ++u) {
+            const int idx = b0 + u * blockDim.x;
+            xs[u] = make_double2(0.0, 0.0);
+            if (idx < n * C) {
+                const int c = idx & (C - 1), i = idx >> logC;
+                const size_t q = q0 + c;
+                if (q < inner) xs[u] = base[(size_t)i * inner + q];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < LB; ++u) {
+            const int idx = b0 + u * blockDim.x;
+            if (idx < n * C) {
+                double2 x = xs[u];
+                if (inverse) x.y = -x.y;   /* inverse DFT = conj(DFT(conj(x))) */
+                a[(idx >> logC) * C + (idx & (C - 1))] = x;
+            }
+        }
     }
     __syncthreads();
     const double2 *z = fft_smem(a, b, pl, C, tw);
@@ -384,12 +418,23 @@ __global__ void __launch_bounds__(FFT_T) k_bins(BinConst bc, const double2 *__re
 }
 
 /* Fixed-order sum of the per-block histograms. */
-__global__ void k_bins_reduce(const double *__restrict__ hist, int nblk, int width, double *out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= width) return;
+__global__ void __launch_bounds__(256) k_bins_reduce(const double *__restrict__ hist, int nblk, int width,
+                                                     double *out) {
+    /* 32 columns per block; warp w adds the rows w, w + 8, ... of its lane's
+     * column, then the 8 warp sums are added in warp order (fixed order) */
+    __shared__ double part[8][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i = blockIdx.x * 32 + lane;
     double s = 0.0;
-    for (int b = 0; b < nblk; ++b) s = __dadd_rn(s, hist[(size_t)b * width + i]);
-    out[i] = s;
+    if (i < width)
+        for (int b = warp; b < nblk; b += 8) s = __dadd_rn(s, __ldcg(&hist[(size_t)b * width + i]));
+    part[warp][lane] = s;
+    __syncthreads();
+    if (warp == 0 && i < width) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t = __dadd_rn(t, part[w][lane]);
+        out[i] = t;
+    }
 }
 
 Plan plan_of(const FftState &f) {
@@ -565,7 +610,7 @@ cudaError_t fft_bins(FftState *f, double L, cudaStream_t s) {
     k_bins<<<f->hist_blocks, FFT_T, sm, s>>>(bc, f->half, f->hist);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int width = 3 * bc.nbins;
-    k_bins_reduce<<<(width + 255) / 256, 256, 0, s>>>(f->hist, f->hist_blocks, width, f->bins_out);
+    k_bins_reduce<<<(width + 31) / 32, 256, 0, s>>>(f->hist, f->hist_blocks, width, f->bins_out);
     return cudaGetLastError();
 }
 
