@@ -14,6 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libcoolbubble_b200.so")
 
 CB_OK, CB_EINVAL, CB_ENOMEM, CB_EDEVICE, CB_ETIMEOUT, CB_EUNSUPPORTED, CB_EBUSY, CB_ENOTFOUND = 0, -1, -2, -3, -4, -5, -6, -7
+CB_EIO = -8
 CB_FP64, CB_FP32C = 0, 1
 CB_STEP_SUMS, CB_STEP_LOCAL = 1, 2
 
@@ -84,6 +85,10 @@ _SIGS = {
     "cb_dft_c2r": (C.c_int, [C.c_int, C.c_int, _dp, _dp]),
     "cb_initial_condition": (C.c_int, [C.POINTER(cb_params), C.POINTER(cb_ic_params), C.c_char_p, _dp, _dp,
                                        C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "cb_h5_write_floats": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int,
+                                     C.POINTER(C.c_char_p), C.POINTER(_fp), C.c_int, C.POINTER(C.c_char_p), _dp,
+                                     C.c_int, C.c_int]),
+    "cb_out_field": (C.c_int, [_h, C.c_char_p, C.c_int]),
     "cb_destroy": (C.c_int, [_h]),
     "cb_step_static_noalloc": (C.c_int, [C.POINTER(cb_params), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_double, C.POINTER(cb_sums)]),

@@ -12,6 +12,8 @@ Everything site-level runs on the GPU; this class only moves arguments.
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 from . import _lib as L
@@ -130,6 +132,12 @@ class Bubble:
         out = np.empty(count)
         check(L.lib.cb_get_line(self._h, int(i0), int(i1), int(i2), count, L.dptr(out)), self._h)
         return out
+
+    def OutField(self, path, threads=0):
+        """Write the snapshot file <path> as Bubble::OutField does (bubble.cpp:887-953):
+        an HDF5 file with phi, pi (and Ekin, gradphi, potEnergy when memorysave == 0),
+        written by the library without libhdf5 (cb_out_field)."""
+        check(L.lib.cb_out_field(self._h, os.fsencode(path), int(threads)), self._h)
 
     @property
     def phi(self):

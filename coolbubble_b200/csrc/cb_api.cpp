@@ -37,6 +37,7 @@ const char *status_text(int s) {
         case CB_EUNSUPPORTED: return "unsupported";
         case CB_EBUSY: return "busy";
         case CB_ENOTFOUND: return "not found";
+        case CB_EIO: return "file could not be written";
     }
     return "unknown status";
 }

@@ -198,47 +198,16 @@ void parameters_file(const Run &r) {
     std::fclose(fp);
 }
 
-/* bubble.cpp:887-954: datasets phi, pi (and Ekin, gradphi, potEnergy) as float,
- * attributes D, L, nGrids, reduc, c, t, a (manifest + raw payload layout). */
+/* bubble.cpp:887-954: the HDF5 snapshot (datasets phi, pi and, with
+ * memorysave == 0, Ekin, gradphi, potEnergy; attributes D, L, nGrids, reduc,
+ * c, t, a), written by the library's own HDF5 writer */
 bool snapshot(Run &r, int n) {
     const Options &o = r.o;
     std::cout << "snapshot " << n << " at t = " << r.line.t << std::endl;
-    std::vector<float> phi(r.N), pi(r.N), ek, eg, ep;
-    if (o.memorysave == 0) { ek.resize(r.N); eg.resize(r.N); ep.resize(r.N); }
-    int st = cb_get_fields_f32(r.h, phi.data(), pi.data(), o.memorysave == 0 ? ek.data() : nullptr,
-                               o.memorysave == 0 ? eg.data() : nullptr, o.memorysave == 0 ? ep.data() : nullptr);
-    if (st != CB_OK) return r.fail(st, "downloading a snapshot");
-    int reduc = 1;
-    if (o.D == 2 && o.nGrids > 2048) reduc = o.nGrids / 2048;
-    if (o.D == 3 && o.nGrids > 512) reduc = o.nGrids / 512;
-    const int m = (o.nGrids + reduc - 1) / reduc;
     const std::string path = r.folder + "/_phi_t=" + four(n) + ".h5";
-    std::vector<std::pair<std::string, std::vector<float> *>> sets = {{"phi", &phi}, {"pi", &pi}};
-    if (o.memorysave != 1) sets.insert(sets.end(), {{"Ekin", &ek}, {"gradphi", &eg}, {"potEnergy", &ep}});
-    FILE *man = std::fopen(path.c_str(), "w");
-    if (!man) { std::cerr << "Error: could not write the snapshot " << path << std::endl; return true; }
-    const int n0 = o.D >= 3 ? o.nGrids : 1, n1 = o.D >= 2 ? o.nGrids : 1;
-    for (auto &ds : sets) {
-        std::fprintf(man, "dataset %s %d", ds.first.c_str(), o.D);
-        for (int a = 0; a < o.D; ++a) std::fprintf(man, " %d", m);
-        std::fprintf(man, "\n");
-        std::vector<float> thin;
-        thin.reserve((size_t)std::pow((double)m, o.D));
-        for (int i0 = 0; i0 < n0; i0 += (o.D >= 3 ? reduc : 1))
-            for (int i1 = 0; i1 < n1; i1 += (o.D >= 2 ? reduc : 1))
-                for (int i2 = 0; i2 < o.nGrids; i2 += reduc)
-                    thin.push_back((*ds.second)[((size_t)i0 * n1 + i1) * o.nGrids + i2]);
-        FILE *f = std::fopen((path + "." + ds.first + ".f32").c_str(), "wb");
-        if (f) {
-            std::fwrite(thin.data(), sizeof(float), thin.size(), f);
-            std::fclose(f);
-        }
-    }
-    const std::pair<const char *, double> attrs[] = {{"D", (double)o.D}, {"L", o.L}, {"nGrids", (double)o.nGrids},
-                                                     {"reduc", (double)reduc}, {"c", o.c}, {"t", r.line.t},
-                                                     {"a", r.line.a}};
-    for (auto &at : attrs) std::fprintf(man, "attr %s %.17g\n", at.first, at.second);
-    std::fclose(man);
+    int st = cb_out_field(r.h, path.c_str(), 0);
+    if (st == CB_EIO) std::cerr << "Error: could not write the snapshot " << path << std::endl;   /* bubble.cpp:950-952 */
+    else if (st != CB_OK) return r.fail(st, "writing a snapshot");
     /* bubble.cpp:642-709: the power spectrum file */
     const int nb = cb_nbins(o.D, o.nGrids);
     std::vector<double> pw(nb), ws(nb), ks(nb);

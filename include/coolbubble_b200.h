@@ -37,6 +37,7 @@ extern "C" {
 #define CB_EUNSUPPORTED (-5) /* valid request this build does not handle */
 #define CB_EBUSY (-6)        /* no room now (pool admission) */
 #define CB_ENOTFOUND (-7)    /* unknown run id */
+#define CB_EIO (-8)          /* a file could not be written */
 
 /* ---- precision of the evolved fields --------------------------------- */
 #define CB_FP64 0   /* double fields and arithmetic: the parity path */
@@ -138,6 +139,29 @@ int cb_pinned_free(void *p);
  * its bounded waits ran out (the kernel then returned without finishing the
  * step; calls that read the device state report CB_ETIMEOUT). */
 int cb_device_error(cb_handle *h, int *code);
+
+/* ---- field snapshots as HDF5 files ------------------------------------ */
+/* Writes float datasets of one shape, chunked, byte-shuffled and deflated,
+ * and scalar double attributes on the root group, as an HDF5 file in the
+ * format libhdf5 writes by default (superblock version 0), without libhdf5.
+ * Replaces the HDF5 C++ calls of Bubble::OutField (bubble.cpp:919-953:
+ * H5File, DataSpace, DSetCreatPropList::setChunk/setShuffle/setDeflate,
+ * createDataSet(...).write, createAttribute(...).write).
+ *   rank 1..3; dims, chunk: rank sizes, 1 <= chunk <= dims; data[s]: the
+ *   product of dims floats in row-major order; nsets <= 8; deflate_level
+ *   0..9; threads <= 0: all host threads (the bytes written do not depend
+ *   on it). CB_EIO when the file cannot be written. */
+int cb_h5_write_floats(const char *path, int rank, const int64_t *dims, const int64_t *chunk, int nsets,
+                       const char *const *names, const float *const *data, int nattrs,
+                       const char *const *attr_names, const double *attr_values, int deflate_level, int threads);
+
+/* Bubble::OutField (bubble.cpp:887-953) in full: downloads phi, pi (and the
+ * local energy arrays when memorysave == 0) as float, thins lattices above
+ * 2048^2 / 512^3 to every reduc-th point, and writes <path> with the
+ * reference's datasets (phi, pi, Ekin, gradphi, potEnergy), chunking
+ * (1-D whole field, 2-D min(n, max(1, 65536 / n)) rows, 3-D planes), filters
+ * (shuffle, deflate 9) and attributes (D, L, nGrids, reduc, c, t, a). */
+int cb_out_field(cb_handle *h, const char *path, int threads);
 
 /* The latest scalars (t, a, a', H, C and the last measured sums). */
 int cb_get_sums(cb_handle *h, cb_sums *out);

@@ -11,6 +11,8 @@ import tempfile
 import numpy as np
 import pytest
 
+import h5read
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 EXE = os.path.join(ROOT, "coolbubble_b200", "lib", "coolbubble_gpu")
 GOLD = os.path.join(ROOT, "tests", "golden", "run_d2")
@@ -50,6 +52,27 @@ def _numbers(path, skip_comments=True):
     return rows
 
 
+def _check_snapshot_file(mine, manifest):
+    """This build's HDF5 snapshot against the manifest the reference's OutField
+    left (datasets with their shapes, attributes with their values), plus the
+    storage settings OutField asks for (bubble.cpp:936-943)."""
+    f = h5read.File(mine)
+    lines = [ln.split() for ln in open(manifest).read().splitlines() if ln.strip()]
+    sets = {ln[1]: tuple(int(x) for x in ln[3:]) for ln in lines if ln[0] == "dataset"}
+    attrs = {ln[1]: float(ln[2]) for ln in lines if ln[0] == "attr"}
+    assert sorted(f.keys()) == sorted(sets)
+    for name, shape in sets.items():
+        d = f[name]
+        assert d.shape == shape and d.dtype == np.float32
+        D, m = len(shape), shape[0]
+        chunk = {1: (m,), 2: (min(m, max(1, 65536 // m)), m), 3: (1, m, m)}[D]
+        assert d.kind == "chunked" and d.chunks == chunk
+        assert [(x["name"], x["cd"]) for x in d.filters] == [("shuffle", [4]), ("deflate", [9])]
+    assert sorted(f.attrs) == sorted(attrs)
+    for k, v in attrs.items():
+        assert float(f.attrs[k]) == pytest.approx(v, rel=1e-14, abs=1e-300)
+
+
 @pytest.mark.gpu
 def test_run_folder_matches_reference_executable():
     meta = json.load(open(os.path.join(GOLD, "args.json")))
@@ -82,18 +105,15 @@ def test_run_folder_matches_reference_executable():
                 for ra, rb in zip(A, B):                            # printed with 6 significant digits
                     np.testing.assert_allclose(ra, rb, rtol=2e-6, atol=1e-300)
             elif fn.endswith(".f32"):
-                A, B = np.fromfile(a, dtype=np.float32), np.fromfile(b, dtype=np.float32)
+                # the reference's dataset payload (HDF5 stand-in of the oracle build) against
+                # the same dataset of this build's HDF5 file
+                h5name, ds = fn[:-len(".f32")].rsplit(".", 1)
+                A = h5read.File(os.path.join(mine, h5name))[ds][:].ravel()
+                B = np.fromfile(b, dtype=np.float32)
                 assert A.shape == B.shape
                 np.testing.assert_allclose(A, B, rtol=2e-7, atol=1e-12 * max(np.abs(B).max(), 1e-30))
             elif fn.endswith(".h5"):
-                la, lb = open(a).read().split("\n"), open(b).read().split("\n")
-                assert len(la) == len(lb)
-                for x, y in zip(la, lb):
-                    if x.startswith("attr "):
-                        assert x.split()[1] == y.split()[1]
-                        assert float(x.split()[2]) == pytest.approx(float(y.split()[2]), rel=1e-14, abs=1e-300)
-                    else:
-                        assert x == y
+                _check_snapshot_file(a, b)
 
 
 @pytest.mark.gpu
