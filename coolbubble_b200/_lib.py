@@ -89,6 +89,8 @@ _SIGS = {
                                      C.POINTER(C.c_char_p), C.POINTER(_fp), C.c_int, C.POINTER(C.c_char_p), _dp,
                                      C.c_int, C.c_int]),
     "cb_out_field": (C.c_int, [_h, C.c_char_p, C.c_int]),
+    "cb_out_field_async": (C.c_int, [_h, C.c_char_p, C.c_int]),
+    "cb_out_field_wait": (C.c_int, [_h]),
     "cb_destroy": (C.c_int, [_h]),
     "cb_step_static_noalloc": (C.c_int, [C.POINTER(cb_params), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_double, C.POINTER(cb_sums)]),

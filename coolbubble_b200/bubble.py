@@ -133,11 +133,18 @@ class Bubble:
         check(L.lib.cb_get_line(self._h, int(i0), int(i1), int(i2), count, L.dptr(out)), self._h)
         return out
 
-    def OutField(self, path, threads=0):
+    def OutField(self, path, threads=0, background=False):
         """Write the snapshot file <path> as Bubble::OutField does (bubble.cpp:887-953):
         an HDF5 file with phi, pi (and Ekin, gradphi, potEnergy when memorysave == 0),
-        written by the library without libhdf5 (cb_out_field)."""
-        check(L.lib.cb_out_field(self._h, os.fsencode(path), int(threads)), self._h)
+        written by the library without libhdf5 (cb_out_field). With background=True
+        the call returns once the fields are on the host and the file is written on a
+        library thread; OutFieldWait() collects it."""
+        fn = L.lib.cb_out_field_async if background else L.lib.cb_out_field
+        check(fn(self._h, os.fsencode(path), int(threads)), self._h)
+
+    def OutFieldWait(self):
+        """Wait for a background OutField; raises CBError if its file could not be written."""
+        check(L.lib.cb_out_field_wait(self._h), self._h)
 
     @property
     def phi(self):

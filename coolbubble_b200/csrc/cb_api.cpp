@@ -278,6 +278,7 @@ int alloc_handle(const cb_params *p, cb_handle **out) {
 
 void destroy_handle(cb_handle *h) {
     if (!h) return;
+    finish_writer(h);
     /* every release is ordered after the run's queued work on its own stream */
     auto dfree = [&](void *p) {
         if (p) cudaFreeAsync(p, h->stream);

@@ -143,6 +143,7 @@ struct Run {
     double DeltaV = 1.0;
     size_t N = 0;
     Wall wall;
+    std::string writing;   /* the snapshot whose write is in flight */
     bool fail(int st, const char *what) {
         std::cerr << "Error: " << what << ": " << cb_last_error(h) << " (" << cb_status_string(st) << ")\n";
         return false;
@@ -198,16 +199,29 @@ void parameters_file(const Run &r) {
     std::fclose(fp);
 }
 
+/* Collects the snapshot write in flight; a file that could not be written is
+ * reported and the run carries on, as in bubble.cpp:948-952. */
+bool collect_snapshot(Run &r) {
+    if (r.writing.empty()) return true;
+    const int st = cb_out_field_wait(r.h);
+    if (st == CB_EIO) std::cerr << "Error: could not write the snapshot " << r.writing << std::endl;
+    else if (st != CB_OK) return r.fail(st, "writing a snapshot");
+    r.writing.clear();
+    return true;
+}
+
 /* bubble.cpp:887-954: the HDF5 snapshot (datasets phi, pi and, with
  * memorysave == 0, Ekin, gradphi, potEnergy; attributes D, L, nGrids, reduc,
- * c, t, a), written by the library's own HDF5 writer */
+ * c, t, a), written by the library's own HDF5 writer in the background while
+ * the run goes on (the fields are copied first) */
 bool snapshot(Run &r, int n) {
     const Options &o = r.o;
     std::cout << "snapshot " << n << " at t = " << r.line.t << std::endl;
     const std::string path = r.folder + "/_phi_t=" + four(n) + ".h5";
-    int st = cb_out_field(r.h, path.c_str(), 0);
-    if (st == CB_EIO) std::cerr << "Error: could not write the snapshot " << path << std::endl;   /* bubble.cpp:950-952 */
-    else if (st != CB_OK) return r.fail(st, "writing a snapshot");
+    if (!collect_snapshot(r)) return false;
+    int st = cb_out_field_async(r.h, path.c_str(), 0);
+    if (st != CB_OK) return r.fail(st, "writing a snapshot");
+    r.writing = path;
     /* bubble.cpp:642-709: the power spectrum file */
     const int nb = cb_nbins(o.D, o.nGrids);
     std::vector<double> pw(nb), ws(nb), ks(nb);
@@ -420,6 +434,7 @@ int main(int argc, char **argv) {
         if (next % progress == 0)
             std::cout << "step " << next << " / " << o.nt << " (" << 100 * next / o.nt << "%)" << std::endl;
     }
+    if (!collect_snapshot(r)) return 1;
     cb_destroy(r.h);
     const auto end = std::chrono::high_resolution_clock::now();
     const double el = std::chrono::duration<double>(end - start).count();

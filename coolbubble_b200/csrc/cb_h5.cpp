@@ -39,7 +39,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "coolbubble_b200.h"
@@ -488,7 +490,72 @@ int write_file(const char *path, const Geometry &g, int nsets, const char *const
     return CB_OK;
 }
 
+/* OutField's datasets and attributes, on the host, ready to write */
+int prepare_snapshot(cb_handle *h, const char *path, int threads, cb::Snapshot &snap) {
+    const int D = h->p.d, n = h->p.n_grids;
+    /* bubble.cpp:891-895: thinning of large lattices */
+    int reduc = 1;
+    if (D == 2 && n > 2048) reduc = n / 2048;
+    if (D == 3 && n > 512) reduc = n / 512;
+    const int m = (n + reduc - 1) / reduc;
+    const bool local = h->p.memorysave != 1;
+    auto &full = snap.fields;
+    full.assign(local ? 5 : 2, std::vector<float>(h->N));
+    int r = cb_get_fields_f32(h, full[0].data(), full[1].data(), local ? full[2].data() : nullptr,
+                              local ? full[3].data() : nullptr, local ? full[4].data() : nullptr);
+    if (r != CB_OK) return r;
+    if (reduc > 1) {
+        /* bubble.cpp:905-915: every reduc-th point per axis, in lattice order */
+        const size_t n0 = D >= 3 ? (size_t)n : 1, n1 = D >= 2 ? (size_t)n : 1;
+        const size_t s0 = D >= 3 ? reduc : 1, s1 = D >= 2 ? reduc : 1;
+        for (auto &v : full) {
+            size_t count = 0;
+            for (size_t i0 = 0; i0 < n0; i0 += s0)
+                for (size_t i1 = 0; i1 < n1; i1 += s1)
+                    for (size_t i2 = 0; i2 < (size_t)n; i2 += reduc) v[count++] = v[(i0 * n1 + i1) * n + i2];
+            v.resize(count);
+            v.shrink_to_fit();
+        }
+    }
+    /* bubble.cpp:934-940: shape (m,)*D; chunks of the whole field (1-D), rows (2-D), planes (3-D) */
+    snap.D = D;
+    for (int a = 0; a < 3; ++a) snap.dims[a] = snap.chunk[a] = m;
+    if (D == 2) snap.chunk[0] = std::min<int64_t>(m, std::max<int64_t>(1, 65536 / m));
+    if (D == 3) snap.chunk[0] = 1;
+    cb_sums s;
+    if ((r = cb_get_sums(h, &s)) != CB_OK) return r;
+    /* bubble.cpp:945-951: D, L, nGrids, reduc, c, t, a */
+    const double av[7] = {(double)D, h->p.L, (double)n, (double)reduc, h->p.c, s.t, s.a};
+    std::copy(av, av + 7, snap.attrs);
+    snap.path = path;
+    snap.threads = threads;
+    return CB_OK;
+}
+
+int write_snapshot(const cb::Snapshot &snap, std::string &err) {
+    static const char *names[5] = {"phi", "pi", "Ekin", "gradphi", "potEnergy"};
+    static const char *an[7] = {"D", "L", "nGrids", "reduc", "c", "t", "a"};
+    const float *data[5];
+    for (size_t f = 0; f < snap.fields.size(); ++f) data[f] = snap.fields[f].data();
+    const int r = cb_h5_write_floats(snap.path.c_str(), snap.D, snap.dims, snap.chunk, (int)snap.fields.size(),
+                                     names, data, 7, an, snap.attrs, 9, snap.threads);
+    if (r != CB_OK) err = cb_last_error(nullptr);
+    return r;
+}
+
 }  // namespace
+
+namespace cb {
+int finish_writer(cb_handle *h) {
+    if (!h->writer) return CB_OK;
+    if (h->writer->th.joinable()) h->writer->th.join();
+    const int r = h->writer->status;
+    const std::string e = h->writer->err;
+    delete h->writer;
+    h->writer = nullptr;
+    return r == CB_OK ? CB_OK : fail(h, r, e);
+}
+}  // namespace cb
 
 extern "C" {
 
@@ -528,44 +595,37 @@ int cb_h5_write_floats(const char *path, int rank, const int64_t *dims, const in
 
 int cb_out_field(cb_handle *h, const char *path, int threads) {
     if (!h || !path) return fail(h, CB_EINVAL, "handle and path must not be NULL");
-    const int D = h->p.d, n = h->p.n_grids;
-    /* bubble.cpp:891-895: thinning of large lattices */
-    int reduc = 1;
-    if (D == 2 && n > 2048) reduc = n / 2048;
-    if (D == 3 && n > 512) reduc = n / 512;
-    const int m = (n + reduc - 1) / reduc;
-    const bool local = h->p.memorysave != 1;
-    std::vector<std::vector<float>> full(local ? 5 : 2, std::vector<float>(h->N));
-    int r = cb_get_fields_f32(h, full[0].data(), full[1].data(), local ? full[2].data() : nullptr,
-                              local ? full[3].data() : nullptr, local ? full[4].data() : nullptr);
+    if (h->writer) return fail(h, CB_EBUSY, "a snapshot write is in flight (cb_out_field_wait first)");
+    cb::Snapshot snap;
+    int r = prepare_snapshot(h, path, threads, snap);
     if (r != CB_OK) return r;
-    if (reduc > 1) {
-        /* bubble.cpp:905-915: every reduc-th point per axis, in lattice order */
-        const size_t n0 = D >= 3 ? (size_t)n : 1, n1 = D >= 2 ? (size_t)n : 1;
-        const size_t s0 = D >= 3 ? reduc : 1, s1 = D >= 2 ? reduc : 1;
-        for (auto &v : full) {
-            size_t count = 0;
-            for (size_t i0 = 0; i0 < n0; i0 += s0)
-                for (size_t i1 = 0; i1 < n1; i1 += s1)
-                    for (size_t i2 = 0; i2 < (size_t)n; i2 += reduc) v[count++] = v[(i0 * n1 + i1) * n + i2];
-            v.resize(count);
-        }
+    std::string err;
+    r = write_snapshot(snap, err);
+    return r == CB_OK ? CB_OK : fail(h, r, err);
+}
+
+int cb_out_field_async(cb_handle *h, const char *path, int threads) {
+    if (!h || !path) return fail(h, CB_EINVAL, "handle and path must not be NULL");
+    if (h->writer) return fail(h, CB_EBUSY, "a snapshot write is in flight (cb_out_field_wait first)");
+    auto snap = std::make_shared<cb::Snapshot>();
+    /* leave one host thread to the caller, who keeps launching steps */
+    if (threads <= 0) threads = std::max(1, omp_get_max_threads() - 1);
+    int r = prepare_snapshot(h, path, threads, *snap);
+    if (r != CB_OK) return r;
+    auto *w = new cb::SnapshotWriter;
+    try {
+        w->th = std::thread([w, snap] { w->status = write_snapshot(*snap, w->err); });
+    } catch (...) {
+        delete w;
+        return fail(h, CB_ENOMEM, "cannot start the snapshot writer thread");
     }
-    /* bubble.cpp:934-940: shape (m,)*D; chunks of the whole field (1-D), rows (2-D), planes (3-D) */
-    int64_t dims[3] = {m, m, m}, chunk[3] = {m, m, m};
-    if (D == 2) chunk[0] = std::min<int64_t>(m, std::max<int64_t>(1, 65536 / m));
-    if (D == 3) chunk[0] = 1;
-    const char *names[5] = {"phi", "pi", "Ekin", "gradphi", "potEnergy"};
-    const float *data[5];
-    for (size_t f = 0; f < full.size(); ++f) data[f] = full[f].data();
-    cb_sums s;
-    if ((r = cb_get_sums(h, &s)) != CB_OK) return r;
-    /* bubble.cpp:945-951 */
-    const char *an[7] = {"D", "L", "nGrids", "reduc", "c", "t", "a"};
-    const double av[7] = {(double)D, h->p.L, (double)n, (double)reduc, h->p.c, s.t, s.a};
-    r = cb_h5_write_floats(path, D, dims, chunk, (int)full.size(), names, data, 7, an, av, 9, threads);
-    if (r != CB_OK) return fail(h, r, cb_last_error(nullptr));
+    h->writer = w;
     return CB_OK;
+}
+
+int cb_out_field_wait(cb_handle *h) {
+    if (!h) return fail(nullptr, CB_EINVAL, "handle is NULL");
+    return cb::finish_writer(h);
 }
 
 }  // extern "C"

@@ -5,12 +5,28 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "cb_internal.h"
 #include "coolbubble_b200.h"
 
 namespace cb {
 struct FftState;
+/* OutField's datasets and attributes on the host, ready to write (cb_h5.cpp) */
+struct Snapshot {
+    std::string path;
+    int D = 0, threads = 0;
+    int64_t dims[3] = {1, 1, 1}, chunk[3] = {1, 1, 1};
+    std::vector<std::vector<float>> fields;
+    double attrs[7] = {};
+};
+/* a snapshot write running on a host thread (cb_out_field_async) */
+struct SnapshotWriter {
+    std::thread th;
+    int status = 0;
+    std::string err;
+};
 }
 
 struct cb_handle {
@@ -37,6 +53,7 @@ struct cb_handle {
     bool pending = false;   /* drift-first: phi is one drift behind the whole step */
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cb::FftState *fft = nullptr;
+    cb::SnapshotWriter *writer = nullptr;
     std::string err;
 };
 
@@ -48,6 +65,7 @@ int flush_pending(cb_handle *h);
 int ensure_tmp(cb_handle *h, size_t bytes);
 void destroy_handle(cb_handle *h);
 void free_fft(cb_handle *h);
+int finish_writer(cb_handle *h);   /* waits for a snapshot write in flight; its status */
 int step_impl(cb_handle *h, int nsteps, int flags, bool timed);
 int enqueue_record_copy(cb_handle *h, DevState *dst);
 int sums_from_record(cb_handle *h, const DevState &s, double t, cb_sums *out);

@@ -163,6 +163,16 @@ int cb_h5_write_floats(const char *path, int rank, const int64_t *dims, const in
  * (shuffle, deflate 9) and attributes (D, L, nGrids, reduc, c, t, a). */
 int cb_out_field(cb_handle *h, const char *path, int threads);
 
+/* Same file, written in the background: returns once the fields are on the
+ * host; compression and writing continue on a library thread (threads <= 0:
+ * all host threads but one) while the caller keeps stepping. One write in
+ * flight per handle: cb_out_field / cb_out_field_async return CB_EBUSY until
+ * cb_out_field_wait has collected it. cb_out_field_wait returns that write's
+ * status (CB_EIO if the file could not be written; CB_OK if none was in
+ * flight). cb_destroy waits for a write in flight. */
+int cb_out_field_async(cb_handle *h, const char *path, int threads);
+int cb_out_field_wait(cb_handle *h);
+
 /* The latest scalars (t, a, a', H, C and the last measured sums). */
 int cb_get_sums(cb_handle *h, cb_sums *out);
 

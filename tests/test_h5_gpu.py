@@ -65,3 +65,44 @@ def test_out_field_thins_large_2d_lattices(tmp_path):
     assert f.attrs["reduc"] == 2 and f.attrs["nGrids"] == n
     assert f["phi"].shape == (m, m) and f["phi"].chunks == _reference_chunks(2, m) == (31, m)
     assert f["phi"][:].tobytes() == phi[::2, ::2].tobytes()
+
+
+def test_background_write_overlaps_steps(tmp_path):
+    """cb_out_field_async: the file holds the fields of the call's time even though
+    the run steps on while it is written; one write in flight per handle."""
+    from coolbubble_b200 import CBError
+    from coolbubble_b200 import _lib as L
+    s = _bubble(3, 64, "fp32c", 0, seed=2)
+    s.step(2, sums=True, local=True)
+    ref = s.fields_f32()
+    t0 = s.sums()["t"]
+    s.OutField(tmp_path / "a.h5", background=True)
+    with pytest.raises(CBError) as e:
+        s.OutField(tmp_path / "b.h5")
+    assert e.value.status == L.CB_EBUSY
+    s.step(5, sums=True)
+    s.OutFieldWait()
+    s.OutFieldWait()                                  # nothing in flight: OK
+    s.OutField(tmp_path / "c.h5", background=True)   # collected by close()
+    later = s.fields_f32(local=False)
+    s.close()
+    f = h5read.File(str(tmp_path / "a.h5"))
+    assert f["phi"][:].ravel().tobytes() == ref["phi"].tobytes()
+    assert f["potEnergy"][:].ravel().tobytes() == ref["epot"].tobytes()
+    assert float(f.attrs["t"]) == t0
+    g = h5read.File(str(tmp_path / "c.h5"))
+    assert g["phi"][:].ravel().tobytes() == later["phi"].tobytes()
+    assert not (tmp_path / "b.h5").exists()
+
+
+def test_background_write_error_is_reported_by_wait(tmp_path):
+    from coolbubble_b200 import CBError
+    from coolbubble_b200 import _lib as L
+    s = _bubble(2, 64, "fp32c", 1)
+    s.OutField(tmp_path / "missing-dir" / "x.h5", background=True)
+    with pytest.raises(CBError) as e:
+        s.OutFieldWait()
+    assert e.value.status == L.CB_EIO
+    s.OutField(tmp_path / "ok.h5")                   # the handle is usable afterwards
+    s.close()
+    assert sorted(h5read.File(str(tmp_path / "ok.h5")).keys()) == ["phi", "pi"]
