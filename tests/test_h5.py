@@ -201,3 +201,62 @@ def test_duplicate_and_too_many_datasets(tmp_path):
     assert st == L.CB_EINVAL and b"twice" in L.lib.cb_last_error(None)
     with pytest.raises(CBError):
         write_floats(tmp_path / "m.h5", {"x%d" % i: a for i in range(9)}, (4,))
+
+
+def _h5py_stand_in():
+    """The part of h5py that the reference's reader uses (File as a context
+    manager, `name in f`, f[name][:], f.attrs), over the strict test reader."""
+    import types
+
+    class _File:
+        def __init__(self, path, mode="r"):
+            assert mode == "r"
+            self._f = h5read.File(str(path))
+            self.attrs = self._f.attrs
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *exc):
+            return False
+
+        def __contains__(self, name):
+            return name in self._f
+
+        def __getitem__(self, name):
+            return self._f[name]
+
+    mod = types.ModuleType("h5py")
+    mod.File = _File
+    return mod
+
+
+def test_reference_reader_opens_the_snapshots(tmp_path, monkeypatch):
+    """The reference's own snapshot reader (python/runfiles.py, read_snapshot)
+    on files with OutField's layout written by this library: fields, axes from
+    the stored thinning stride, t and a."""
+    import importlib.util
+    import sys
+    ref = os.environ.get("CB_REFERENCE", "/root/reference")
+    src = os.path.join(ref, "python", "runfiles.py")
+    if not os.path.exists(src):
+        pytest.skip("the reference sources are not present")
+    monkeypatch.setitem(sys.modules, "h5py", _h5py_stand_in())
+    spec = importlib.util.spec_from_file_location("reference_runfiles", src)
+    runfiles = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(runfiles)
+    rng = np.random.default_rng(21)
+    for D, n_grids, reduc in [(2, 64, 1), (2, 4100, 2), (3, 16, 1), (1, 40, 1)]:
+        m = -(-n_grids // reduc)
+        shape = (m,) * D
+        chunk = {1: (m,), 2: (min(m, max(1, 65536 // m)), m), 3: (1, m, m)}[D]
+        data = {k: rng.standard_normal(shape).astype(np.float32) for k in ("phi", "pi", "gradphi")}
+        attrs = {"D": D, "L": 16.0, "nGrids": n_grids, "reduc": reduc, "c": 4.0, "t": 2.5, "a": 1.5}
+        p = tmp_path / ("_phi_t=%04d.h5" % n_grids)
+        write_floats(p, data, chunk, attrs)
+        fields, axes, info = runfiles.read_snapshot(p, {"D": D, "L": 16.0, "nGrids": n_grids})
+        for k, v in data.items():
+            assert fields[k].shape == shape and fields[k].tobytes() == v.tobytes()
+        assert info == {"t": 2.5, "a": 1.5, "reduc": float(reduc)}
+        assert len(axes) == D
+        np.testing.assert_allclose(axes[0], (np.arange(m) * reduc + 0.5) * 16.0 / n_grids, rtol=0, atol=0)
