@@ -450,6 +450,22 @@ def run_serving_bench(args):
     return 0
 
 
+def spectrum_ms(s, reps):
+    """Device time of one power spectrum of the run's field (cb_power_spectrum:
+    r2c FFT + shell binning, bubble.cpp:642-709), averaged over reps calls after
+    one untimed call; each call also returns its bins to the host."""
+    if reps <= 0:
+        return None
+    from coolbubble_b200 import _lib as L
+    s.spectrum_sums()
+    L.check(L.lib.cb_timer_start(s._h), s._h)
+    for _ in range(reps):
+        s.spectrum_sums()
+    ms = L.C.c_double()
+    L.check(L.lib.cb_timer_stop(s._h, L.C.byref(ms)), s._h)
+    return ms.value / reps
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -463,6 +479,8 @@ def main():
     ap.add_argument("--slots", type=int, default=64, help="serving: runs on the GPU at once")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (profiling runs)")
+    ap.add_argument("--spectra", type=int, default=5,
+                    help="power spectra timed after the steps (per-snapshot cost; 0: none)")
     args = ap.parse_args()
     if args.workload == "serving":
         if args.impl == "reference":
@@ -512,6 +530,7 @@ def main():
     ms = max_over_ranks(dist, ms)
     clk = clocks.stop()
     final = s.sums()
+    spec_ms = spectrum_ms(s, args.spectra)
     s.close()
     value = N * args.steps * ws / (ms / 1e3)
 
@@ -519,7 +538,7 @@ def main():
         if rank == 0:
             print(json.dumps({"metric": "lattice site-updates/s", "value": value, "unit": "site-updates/s",
                               "ms_per_step": ms / args.steps, "config": {"workload": args.workload},
-                              "quick": True}), flush=True)
+                              "spectrum_ms": spec_ms, "quick": True}), flush=True)
         return 0
 
     # ---- plain FP64 path on the same lattice ----------------------------------
@@ -567,6 +586,8 @@ def main():
         "gpu_launches": launches,
         "clocks": clk,
         "final_etot": final["etot"],
+        # per snapshot, outside the timed steps: one power spectrum of the final field
+        "spectrum_ms": spec_ms,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         v, kind, cores, sample = cpu_sample(w, phi0, pi0, max_steps=20, budget_s=20.0)
