@@ -593,9 +593,11 @@ int sm_count() {
 /* The tiled path covers d = 3 with n a multiple of the vector width, n >= 64
  * and n <= 1024; returns false for other shapes (the generic kernel runs).
  * Geometry: TJ rows per tile (TJ * n about 2048 sites in float, 1024 in
- * double), as many ring stages as keep two blocks per SM (4..6), one block
- * per resident slot (2 per SM), and the number of plane parts that balances
- * the fixed cost of every item against the part-filled last round.
+ * double; one row when a row is longer), as many ring stages as keep two
+ * blocks per SM (4..8) or, when four stages do not fit in half an SM, one
+ * block per SM with up to 8 stages in 220 KB; one block per resident slot,
+ * and the number of plane parts that balances the fixed cost of every item
+ * against the part-filled last round.
  * CB_STEP3_PARTS overrides the parts. */
 bool step3_geometry_parts(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid,
                           int &parts) {
@@ -603,7 +605,7 @@ bool step3_geometry_parts(const StepConst &k, int prec, int &tj, int &nstage, si
     const int n = k.n;
     const int esz = prec == P_FP64 ? 8 : 4;
     const int W = 16 / esz;
-    if (n % W != 0 || n < 64 || n > 1024) return false;
+    if (n % W != 0 || n < 64) return false;
     int tile_sites = prec == P_FP64 ? 1024 : 2048;
     const char *tenv = std::getenv("CB_STEP3_TILE");
     if (tenv && std::atoi(tenv) >= 64) tile_sites = std::atoi(tenv);
@@ -612,14 +614,17 @@ bool step3_geometry_parts(const StepConst &k, int prec, int &tj, int &nstage, si
         if (n % t == 0) tj = t;
     const bool df = k.expanding != 0;
     const size_t stage = ((size_t)(tj + 2) + (size_t)(tj + (df ? 2 : 0))) * n * esz;
-    const size_t budget = 106 * 1024;   /* two blocks per SM, with their static shared memory */
-    nstage = (int)((budget - HDR) / stage);
+    /* two blocks per SM (with their static shared memory) while four stages fit
+     * in half an SM; beyond that (rows of more than about 1000 floats with
+     * drift-first, 1300 without) one block per SM with a deeper ring */
+    const size_t budget2 = 106 * 1024, budget1 = 220 * 1024;
+    const int per_sm = HDR + 4 * stage <= budget2 ? 2 : 1;
+    nstage = (int)(((per_sm == 2 ? budget2 : budget1) - HDR) / stage);
     if (nstage > 8) nstage = 8;
-    if (nstage < 4) nstage = 4;
+    if (nstage < 4) return false;
     smem = HDR + nstage * stage;
-    if (smem > 220 * 1024) return false;
     const long long ntiles = n / tj;
-    const long long slots = 2LL * sm_count();
+    const long long slots = (long long)per_sm * sm_count();
     /* time in units of one plane of one tile. An item costs its planes plus a
      * fixed part -- about one plane for a static background, 2.5 with
      * drift-first (its halo planes are drifted too). Items that fit the slots
