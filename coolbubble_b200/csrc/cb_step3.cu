@@ -608,17 +608,30 @@ bool step3_geometry_parts(const StepConst &k, int prec, int &tj, int &nstage, si
     if (n % W != 0 || n < 64) return false;
     int tile_sites = prec == P_FP64 ? 1024 : 2048;
     const char *tenv = std::getenv("CB_STEP3_TILE");
-    if (tenv && std::atoi(tenv) >= 64) tile_sites = std::atoi(tenv);
-    tj = 1;
-    for (int t = 1; t <= n && t * n <= tile_sites; ++t)
-        if (n % t == 0) tj = t;
+    const bool tile_given = tenv && std::atoi(tenv) >= 64;
+    if (tile_given) tile_sites = std::atoi(tenv);
     const bool df = k.expanding != 0;
-    const size_t stage = ((size_t)(tj + 2) + (size_t)(tj + (df ? 2 : 0))) * n * esz;
-    /* two blocks per SM (with their static shared memory) while four stages fit
-     * in half an SM; beyond that (rows of more than about 1000 floats with
-     * drift-first, 1300 without) one block per SM with a deeper ring */
+    auto stage_of = [&](int t) { return ((size_t)(t + 2) + (size_t)(t + (df ? 2 : 0))) * n * esz; };
+    auto rows_for = [&](int sites, size_t cap) {
+        int best = 0;
+        for (int t = 1; t <= n && (long long)t * n <= sites; ++t)
+            if (n % t == 0 && HDR + 4 * stage_of(t) <= cap) best = t;
+        return best;
+    };
+    /* two blocks per SM (with their static shared memory) while four stages of
+     * the tile fit in half an SM and the tile has more than one row. Else one
+     * block per SM with tiles of twice the sites (the tallest whose four
+     * stages fit in 220 KB) and a deeper ring: a one-row tile stages its two
+     * halo rows (four with drift-first) for every row it computes. */
     const size_t budget2 = 106 * 1024, budget1 = 220 * 1024;
-    const int per_sm = HDR + 4 * stage <= budget2 ? 2 : 1;
+    tj = std::max(1, rows_for(tile_sites, ~size_t(0)));
+    int per_sm = HDR + 4 * stage_of(tj) <= budget2 && (tj > 1 || tile_given) ? 2 : 1;
+    if (per_sm == 1) {
+        const int t1 = rows_for(tile_given ? tile_sites : 2 * tile_sites, budget1);
+        if (t1 == 0) return false;
+        tj = t1;
+    }
+    const size_t stage = stage_of(tj);
     nstage = (int)(((per_sm == 2 ? budget2 : budget1) - HDR) / stage);
     if (nstage > 8) nstage = 8;
     if (nstage < 4) return false;
