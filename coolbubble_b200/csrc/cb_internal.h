@@ -88,6 +88,16 @@ cudaError_t launch_step(int prec, const StepConst &k, bool drift_first, int sums
 /* Number of blocks (and so of partial-sum slots) a step launch may use. */
 size_t step_blocks(const StepConst &k);
 
+/* d = 2 kernel marching column strips down the rows (cb_step2.cu): static
+ * background, n a multiple of the vector width, lattices of at least
+ * STEP2_MIN_SITES sites (below that the generic tile kernel). */
+constexpr size_t STEP2_MIN_SITES = size_t(1) << 20;   /* below 1024^2 both are launch-bound; the tiles win at 128^2 */
+bool step2_applies(const StepConst &k, int prec, bool drift_first);
+size_t step2_blocks(const StepConst &k);
+cudaError_t launch_step2(int prec, const StepConst &k, int sums, const void *phi_in, const void *pi_in,
+                         void *phi_out, void *pi_out, void *le, void *lg, void *lp, DevState *st, double *partials,
+                         cudaStream_t s);
+
 /* d = 3 kernel with TMA-staged row tiles (cb_step3.cu). */
 bool step3_geometry(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid);
 size_t step3_partial_rows(const StepConst &k, int prec);

@@ -438,6 +438,7 @@ size_t step_blocks(const StepConst &k) {
         unsigned g3;
         if (step3_geometry(k, prec, tj, ns, sm, g3)) b = std::max(b, step3_partial_rows(k, prec));
     }
+    if (k.d == 2) b = std::max(b, step2_blocks(k));
     return b;
 }
 
@@ -449,6 +450,8 @@ cudaError_t launch_step(int prec, const StepConst &k, bool drift_first, int sums
     int tj, ns;
     size_t sm;
     unsigned g3;
+    if (step2_applies(k, prec, drift_first))
+        return launch_step2(prec, k, sums, phi_in, pi_in, phi_out, pi_out, loc_ek, loc_eg, loc_ep, st, partials, s);
     if (!k.force_generic && step3_geometry(k, prec, tj, ns, sm, g3))
         return launch_step3(prec, k, drift_first, sums, phi_in, pi_in, phi_out, pi_out, loc_ek, loc_eg, loc_ep, st,
                             partials, s);

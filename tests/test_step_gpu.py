@@ -234,6 +234,39 @@ def test_tiled_kernel_equals_generic_kernel_fp64(case, monkeypatch):
         np.testing.assert_array_equal(fa[key], fb[key])
 
 
+@pytest.mark.parametrize("n,prec", [(1024, "fp64"), (1028, "fp32c"), (2048, "fp32c"), (1032, "fp64"),
+                                    (1026, "fp64"), (4100, "fp32c")])
+def test_strip_kernel_equals_generic_kernel_2d(n, prec, monkeypatch):
+    """The d = 2 strip kernel (column strips marched down the rows; lattices of
+    1024^2 sites and more) does the generic kernel's per-site arithmetic op for
+    op: bit-identical fields and local energy arrays over measured and
+    unmeasured steps; the box sums differ only in their order. Sizes cover rows
+    ending inside a warp (one vector in the last strip) and inside a block,
+    odd vector counts, several strips and bands."""
+    import coolbubble_b200 as cb
+    d, L, c = 2, n / 8.0, 4.0
+    p = cb.make_params(d, n, L, c, 0.1 * L / n, precision=prec)
+    phi0 = bubbles(d, n, L, c, 6, seed=7)
+    pi0 = smooth_noise(d, n, 0.02, seed=8)
+    strip = cb.Bubble(p, phi0, pi0)
+    monkeypatch.setenv("CB_STEP_PATH", "generic")
+    generic = cb.Bubble(p, phi0, pi0)
+    monkeypatch.delenv("CB_STEP_PATH")
+    for steps in (1, 7, 40):
+        a = strip.step(steps, sums=True, local=True)
+        b = generic.step(steps, sums=True, local=True)
+        tol = 1e-13 if prec == "fp64" else 1e-5
+        for key in a:
+            # C = H^2 - Etot / (3 Mpl^2) with H = 0 here: judged on the scale of its terms
+            scale = abs(b["H"]) ** 2 + abs(b["etot"]) / (3 * 200.0 ** 2) if key == "C" else abs(b[key])
+            if key in ("avphi", "avphip"):
+                scale = max(scale, (n ** d * b[key + "_var"]) ** 0.5)
+            assert abs(a[key] - b[key]) <= tol * scale + 1e-300, key
+        fa, fb = strip.fields(), generic.fields()
+        for key in fa:
+            np.testing.assert_array_equal(fa[key], fb[key])
+
+
 def test_fp64_tiled_static_matches_oracle():
     import coolbubble_b200 as cb
     from oracle import bridge as B
