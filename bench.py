@@ -43,6 +43,8 @@ WORKLOADS = {
     "thermal-d3-n256": dict(d=3, n=256, L=32.0, c=2.0, expansion=0, mpl=200.0, precision="fp32c"),
     # expanding background, smaller lattice
     "bubbles-d3-n256-expanding": dict(d=3, n=256, L=32.0, c=4.0, expansion=1, mpl=10.0, precision="fp32c"),
+    # a large 2-D lattice (column-strip kernel), for profiler captures
+    "plain-d2-n8192": dict(d=2, n=8192, L=1024.0, c=4.0, expansion=0, mpl=200.0, precision="fp32c"),
 }
 OUT_ENERGY_EVERY = 40
 BYTES_PER_SITE = {"fp32c": 16, "fp64": 32}   # read + write phi and pi once per step
@@ -450,6 +452,14 @@ def run_serving_bench(args):
     return 0
 
 
+def l2_note(n, d, prec):
+    fields = 2 * n ** d * (4 if prec == "fp32c" else 8)
+    if fields > 126 * 2 ** 20:
+        return "inputs larger than L2 (2 x %d^%d %s = %.2f GiB)" % (n, d, "floats" if prec == "fp32c" else "doubles",
+                                                                      fields / 2 ** 30)
+    return "inputs smaller than L2 (%.0f MiB): L2-resident" % (fields / 2 ** 20)
+
+
 def spectrum_ms(s, reps):
     """Device time of one power spectrum of the run's field (cb_power_spectrum:
     r2c FFT + shell binning, bubble.cpp:642-709), averaged over reps calls after
@@ -568,7 +578,7 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "d": d, "n": n, "L": w["L"], "c": w["c"], "dt": dt,
                    "expansion": w["expansion"], "precision": prec, "parallelism": f"replicas{ws}",
-                   "l2": "inputs larger than L2 (2 x 512^3 floats = 1 GiB)",
+                   "l2": l2_note(n, d, prec),
                    "sums_every": OUT_ENERGY_EVERY, "ic": "seeded gaussian fluctuations, amplitude 0.05",
                    "steps_per_launch": args.steps / launches,
                    "temporal_block": os.environ.get("CB_TEMPORAL_BLOCK", "autotuned")},
