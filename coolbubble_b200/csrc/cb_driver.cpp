@@ -8,10 +8,10 @@
  * 642-709, FullField.dat 993-1006) and the wall tracking of bubble.cpp:535-634
  * (gamma.dat 1009-1015). The compile-time def.h values become
  * options (--dt, --nbubbles, ...) with def.h's defaults. Snapshots are
- * written as a text manifest plus raw float32 payloads per dataset
- * (<file>, <file>.<name>.f32), the layout of the HDF5 stand-in of this
- * repository's oracle; the datasets and attributes are OutField's
- * (bubble.cpp:887-954). Plots and videos are not made.
+ * HDF5 files with OutField's datasets, chunking, filters and attributes
+ * (bubble.cpp:887-954), written by the library's own writer (cb_out_field,
+ * no libhdf5) in the background while the run steps on. Plots and videos
+ * are not made.
  */
 #include <chrono>
 #include <cmath>

@@ -590,8 +590,9 @@ int sm_count() {
     return v;
 }
 
-/* The tiled path covers d = 3 with n a multiple of the vector width, n >= 64
- * and n <= 1024; returns false for other shapes (the generic kernel runs).
+/* The tiled path covers d = 3 with n a multiple of the vector width, n >= 64,
+ * where a ring of four stages fits in 220 KB; returns false for other shapes
+ * (the generic kernel runs).
  * Geometry: TJ rows per tile (TJ * n about 2048 sites in float, 1024 in
  * double; one row when a row is longer), as many ring stages as keep two
  * blocks per SM (4..8) or, when four stages do not fit in half an SM, one
