@@ -279,6 +279,9 @@ int alloc_handle(const cb_params *p, cb_handle **out) {
 void destroy_handle(cb_handle *h) {
     if (!h) return;
     finish_writer(h);
+    for (auto &row : h->graph)
+        for (auto &g : row)
+            if (g) cudaGraphExecDestroy(g);
     /* every release is ordered after the run's queued work on its own stream */
     auto dfree = [&](void *p) {
         if (p) cudaFreeAsync(p, h->stream);
@@ -397,6 +400,60 @@ int choose_temporal(cb_handle *h) {
     return tl;
 }
 
+/* Small lattices: a step's kernel takes less time than its launch, so chains
+ * of GRAPH_STEPS plain steps (no sums reported; an expanding background's
+ * Friedmann update stays on the device) are captured once into a CUDA graph
+ * and replayed. The count is even, so the ping-pong buffers end where they
+ * started and one graph per buffer state serves every chain. Captured in
+ * thread-local mode; if capture or instantiation fails, the handle goes back
+ * to plain launches for good. CB_STEP_GRAPHS=0 turns graphs off. */
+constexpr int GRAPH_STEPS = 16;
+constexpr size_t GRAPH_MAX_SITES = size_t(1) << 22;
+
+bool graphs_wanted(const cb_handle *h) {
+    if (h->graphs_off || h->N > GRAPH_MAX_SITES) return false;
+    const char *e = std::getenv("CB_STEP_GRAPHS");
+    return !(e && std::string(e) == "0");
+}
+
+/* CB_OK: GRAPH_STEPS steps queued; 1: graphs unavailable (launch plainly); < 0: error */
+int replay_step_graph(cb_handle *h) {
+    const int i = h->cphi, j = h->cpi;
+    cudaGraphExec_t &ex = h->graph[i][j];
+    if (!ex) {
+        StepConst k = h->k;
+        k.want_local = 0;
+        const int sums = h->expanding ? 1 : 0;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            h->graphs_off = true;
+            return 1;
+        }
+        int ci = i, cj = j;
+        for (int q = 0; q < GRAPH_STEPS && e == cudaSuccess; ++q) {
+            e = launch_step(h->prec, k, h->expanding, sums, h->phi[ci], h->pi[cj], h->phi[1 - ci], h->pi[1 - cj],
+                            h->loc[0], h->loc[1], h->loc[2], h->st, h->partials, h->stream);
+            ci = 1 - ci;
+            cj = 1 - cj;
+        }
+        const cudaError_t e_end = cudaStreamEndCapture(h->stream, &g);
+        if (e == cudaSuccess) e = e_end;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&ex, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ex = nullptr;
+            h->graphs_off = true;
+            return 1;
+        }
+    }
+    const cudaError_t e = cudaGraphLaunch(ex, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "replaying the step graph");
+    return CB_OK;
+}
+
 int step_impl(cb_handle *h, int nsteps, int flags, bool timed) {
     if (nsteps < 0) return fail(h, CB_EINVAL, "nsteps must be non-negative");
     if ((flags & ~(CB_STEP_SUMS | CB_STEP_LOCAL)) != 0) return fail(h, CB_EINVAL, "unknown flag bits");
@@ -428,6 +485,17 @@ int step_impl(cb_handle *h, int nsteps, int flags, bool timed) {
             h->launches++;
             it += tl;
             continue;
+        }
+        if (plain_left >= GRAPH_STEPS && graphs_wanted(h)) {
+            const int r = replay_step_graph(h);
+            if (r < 0) return r;
+            if (r == CB_OK) {
+                for (int q = 0; q < GRAPH_STEPS; ++q) h->t += h->p.dt;   /* bubble.cpp:871, one addition per step */
+                h->steps_done += GRAPH_STEPS;
+                h->launches += GRAPH_STEPS;
+                it += GRAPH_STEPS;
+                continue;
+            }
         }
         const bool last = it == nsteps;
         const bool local = last && (flags & CB_STEP_LOCAL);

@@ -54,6 +54,9 @@ struct cb_handle {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cb::FftState *fft = nullptr;
     cb::SnapshotWriter *writer = nullptr;
+    /* replayable chains of plain steps (small lattices), by (cphi, cpi) at their start */
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    bool graphs_off = false;
     std::string err;
 };
 

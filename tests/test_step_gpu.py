@@ -267,6 +267,33 @@ def test_strip_kernel_equals_generic_kernel_2d(n, prec, monkeypatch):
             np.testing.assert_array_equal(fa[key], fb[key])
 
 
+@pytest.mark.parametrize("d,n,prec,expansion", [(2, 512, "fp64", 0), (2, 256, "fp32c", 0), (3, 64, "fp32c", 1),
+                                                (3, 64, "fp64", 1), (3, 96, "fp32c", 0), (1, 4096, "fp64", 0)])
+def test_step_graphs_equal_plain_launches(d, n, prec, expansion, monkeypatch):
+    """Chains of plain steps replayed from a CUDA graph (small lattices) queue
+    the same kernels with the same arguments as plain launches: fields, sums,
+    time and launch counts identical, across chains that start from either
+    buffer state and runs whose length is not a multiple of the chain."""
+    import coolbubble_b200 as cb
+    L = n / 8.0
+    p = cb.make_params(d, n, L, 4.0, 0.1 * L / n, expansion=expansion, mpl=10.0, precision=prec, memorysave=0)
+    phi0 = bubbles(d, n, L, 4.0, 4, seed=11) if d > 1 else smooth_noise(d, n, 0.5, seed=11)
+    pi0 = smooth_noise(d, n, 0.02, seed=12)
+    graphed = cb.Bubble(p, phi0, pi0)
+    monkeypatch.setenv("CB_STEP_GRAPHS", "0")
+    plain = cb.Bubble(p, phi0, pi0)
+    for steps in (40, 17, 33, 1, 64):
+        monkeypatch.delenv("CB_STEP_GRAPHS")
+        a = graphed.step(steps, sums=True, local=steps == 64)
+        monkeypatch.setenv("CB_STEP_GRAPHS", "0")
+        b = plain.step(steps, sums=True, local=steps == 64)
+        assert a == b
+    assert graphed.counters() == plain.counters()
+    fa, fb = graphed.fields(), plain.fields()
+    for key in fa:
+        np.testing.assert_array_equal(fa[key], fb[key])
+
+
 def test_fp64_tiled_static_matches_oracle():
     import coolbubble_b200 as cb
     from oracle import bridge as B
