@@ -734,30 +734,32 @@ int cb_get_sums(cb_handle *h, cb_sums *out) {
 }
 
 int cb_get_fields(cb_handle *h, double *phi, double *pi, double *ekin, double *egrad, double *epot) {
-    if (!h) return fail(nullptr, CB_EINVAL, "handle is NULL");
-    if ((ekin || egrad || epot) && h->p.memorysave != 0)
-        return fail(h, CB_EINVAL, "memorysave == 1 keeps no local energy arrays");
-    int r = flush_pending(h);
-    if (r != CB_OK) return r;
-    const void *src[5] = {h->phi[h->cphi], h->pi[h->cpi], h->loc[0], h->loc[1], h->loc[2]};
-    double *dst[5] = {phi, pi, ekin, egrad, epot};
-    std::vector<float> tmp;
-    for (int f = 0; f < 5; ++f) {
-        if (!dst[f]) continue;
-        cudaError_t e;
-        if (h->prec == P_FP64) {
-            e = cudaMemcpyAsync(dst[f], src[f], h->N * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-        } else {
-            tmp.resize(h->N);
-            e = cudaMemcpyAsync(tmp.data(), src[f], h->N * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-            if (e == cudaSuccess)
-                for (size_t i = 0; i < h->N; ++i) dst[f][i] = (double)tmp[i];
+    return cb::guard(h, [&]() -> int {
+        if (!h) return fail(nullptr, CB_EINVAL, "handle is NULL");
+        if ((ekin || egrad || epot) && h->p.memorysave != 0)
+            return fail(h, CB_EINVAL, "memorysave == 1 keeps no local energy arrays");
+        int r = flush_pending(h);
+        if (r != CB_OK) return r;
+        const void *src[5] = {h->phi[h->cphi], h->pi[h->cpi], h->loc[0], h->loc[1], h->loc[2]};
+        double *dst[5] = {phi, pi, ekin, egrad, epot};
+        std::vector<float> tmp;
+        for (int f = 0; f < 5; ++f) {
+            if (!dst[f]) continue;
+            cudaError_t e;
+            if (h->prec == P_FP64) {
+                e = cudaMemcpyAsync(dst[f], src[f], h->N * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+            } else {
+                tmp.resize(h->N);
+                e = cudaMemcpyAsync(tmp.data(), src[f], h->N * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+                if (e == cudaSuccess)
+                    for (size_t i = 0; i < h->N; ++i) dst[f][i] = (double)tmp[i];
+            }
+            if (e != cudaSuccess) return cuda_fail(h, e, "downloading a field");
         }
-        if (e != cudaSuccess) return cuda_fail(h, e, "downloading a field");
-    }
-    return CB_OK;
+        return CB_OK;
+    });
 }
 
 int cb_get_fields_f32(cb_handle *h, float *phi, float *pi, float *ekin, float *egrad, float *epot) {

@@ -500,43 +500,45 @@ int autotune(cb_ensemble::Class &c, cb_handle *h0) {
 extern "C" {
 
 int cb_ensemble_create(int count, cb_handle *const *members, cb_ensemble **out) {
-    if (count < 1 || !members || !out) return fail(nullptr, CB_EINVAL, "cb_ensemble_create: bad arguments");
-    *out = nullptr;
-    cb_ensemble *e = new cb_ensemble();
-    e->members.assign(members, members + count);
-    std::map<long long, int> cls;
-    for (int i = 0; i < count; ++i) {
-        cb_handle *h = members[i];
-        if (!h) { delete e; return fail(nullptr, CB_EINVAL, "cb_ensemble_create: NULL member"); }
-        int cs = h->expanding ? 0 : resident_cluster(h->prec, h->p.d, h->p.n_grids);
-        if (cs > 0 && !cluster_fits(h->prec, cs, resident_smem(h->prec, h->p.n_grids, cs), 256)) cs = 0;
-        if (cs == 0) { e->own.push_back(i); continue; }
-        const long long key = ((long long)h->prec << 40) | ((long long)h->p.n_grids << 8) | cs;
-        auto it = cls.find(key);
-        if (it == cls.end()) {
-            cb_ensemble::Class c;
-            c.prec = h->prec;
-            c.n = h->p.n_grids;
-            c.cs = cs;
-            c.threads = 512;
-            cls[key] = (int)e->classes.size();
-            e->classes.push_back(c);
-            it = cls.find(key);
+    return cb::guard(nullptr, [&]() -> int {
+        if (count < 1 || !members || !out) return fail(nullptr, CB_EINVAL, "cb_ensemble_create: bad arguments");
+        *out = nullptr;
+        cb_ensemble *e = new cb_ensemble();
+        e->members.assign(members, members + count);
+        std::map<long long, int> cls;
+        for (int i = 0; i < count; ++i) {
+            cb_handle *h = members[i];
+            if (!h) { delete e; return fail(nullptr, CB_EINVAL, "cb_ensemble_create: NULL member"); }
+            int cs = h->expanding ? 0 : resident_cluster(h->prec, h->p.d, h->p.n_grids);
+            if (cs > 0 && !cluster_fits(h->prec, cs, resident_smem(h->prec, h->p.n_grids, cs), 256)) cs = 0;
+            if (cs == 0) { e->own.push_back(i); continue; }
+            const long long key = ((long long)h->prec << 40) | ((long long)h->p.n_grids << 8) | cs;
+            auto it = cls.find(key);
+            if (it == cls.end()) {
+                cb_ensemble::Class c;
+                c.prec = h->prec;
+                c.n = h->p.n_grids;
+                c.cs = cs;
+                c.threads = 512;
+                cls[key] = (int)e->classes.size();
+                e->classes.push_back(c);
+                it = cls.find(key);
+            }
+            e->classes[it->second].idx.push_back(i);
         }
-        e->classes[it->second].idx.push_back(i);
-    }
-    for (auto &c : e->classes) {
-        if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaMalloc(&c.dev, c.idx.size() * sizeof(EnsMember)) != cudaSuccess) {
-            cudaGetLastError();
-            cb_ensemble_destroy(e);
-            return fail(nullptr, CB_ENOMEM, "cb_ensemble_create: device allocation failed");
+        for (auto &c : e->classes) {
+            if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaMalloc(&c.dev, c.idx.size() * sizeof(EnsMember)) != cudaSuccess) {
+                cudaGetLastError();
+                cb_ensemble_destroy(e);
+                return fail(nullptr, CB_ENOMEM, "cb_ensemble_create: device allocation failed");
+            }
+            c.threads = autotune(c, members[c.idx[0]]);
         }
-        c.threads = autotune(c, members[c.idx[0]]);
-    }
-    cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming);
-    *out = e;
-    return CB_OK;
+        cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming);
+        *out = e;
+        return CB_OK;
+    });
 }
 
 int cb_ensemble_member_plan(cb_ensemble *e, int m, int *cluster, int *threads) {
@@ -566,107 +568,109 @@ int cb_ensemble_destroy(cb_ensemble *e) {
  * every sums_every-th step are written to out[m * (nsteps / sums_every) + j]
  * (member m, event j); out may be NULL when sums_every == 0. */
 int cb_ensemble_step(cb_ensemble *e, int nsteps, int sums_every, cb_sums *out) {
-    if (!e || nsteps < 0 || sums_every < 0) return fail(nullptr, CB_EINVAL, "cb_ensemble_step: bad arguments");
-    const int nev = sums_every > 0 ? nsteps / sums_every : 0;
-    if (nev > 0 && !out) return fail(nullptr, CB_EINVAL, "cb_ensemble_step: out is NULL");
-    const int count = (int)e->members.size();
-    EnsRecord *drec = nullptr;
-    if (nev > 0 && cudaMalloc(&drec, (size_t)count * nev * sizeof(EnsRecord)) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(nullptr, CB_ENOMEM, "cb_ensemble_step: device allocation of the records failed");
-    }
-    std::vector<double> t_start(count);
-    for (int i = 0; i < count; ++i) t_start[i] = e->members[i]->t;
-    cudaError_t err = cudaSuccess;
-    /* resident classes: one launch each, on their own streams */
-    for (auto &c : e->classes) {
-        std::vector<EnsMember> host(c.idx.size());
-        for (size_t q = 0; q < c.idx.size(); ++q) {
-            cb_handle *h = e->members[c.idx[q]];
-            flush_pending(h);
-            cudaStreamSynchronize(h->stream);
-            host[q].phi = h->phi[h->cphi];
-            host[q].pi = h->pi[h->cpi];
-            host[q].k = h->k;
-            host[q].out_index = c.idx[q] * nev;
-            int ex;
-            host[q].dx_pow2 = std::fabs(std::frexp(h->k.dx, &ex)) == 0.5 ? 1 : 0;
+    return cb::guard(nullptr, [&]() -> int {
+        if (!e || nsteps < 0 || sums_every < 0) return fail(nullptr, CB_EINVAL, "cb_ensemble_step: bad arguments");
+        const int nev = sums_every > 0 ? nsteps / sums_every : 0;
+        if (nev > 0 && !out) return fail(nullptr, CB_EINVAL, "cb_ensemble_step: out is NULL");
+        const int count = (int)e->members.size();
+        EnsRecord *drec = nullptr;
+        if (nev > 0 && cudaMalloc(&drec, (size_t)count * nev * sizeof(EnsRecord)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(nullptr, CB_ENOMEM, "cb_ensemble_step: device allocation of the records failed");
         }
-        err = cudaMemcpyAsync(c.dev, host.data(), host.size() * sizeof(EnsMember), cudaMemcpyHostToDevice, c.stream);
-        if (err == cudaSuccess)
-            err = launch_resident(c.prec, c.dev, (int)c.idx.size(), c.cs, c.threads, nsteps, sums_every, drec,
-                                  resident_smem(c.prec, c.n, c.cs), c.stream);
-        if (err != cudaSuccess) break;
-    }
-    /* the others: their own step kernels on their own streams, records copied on the device */
-    for (int i : e->own) {
-        if (err != cudaSuccess) break;
-        cb_handle *h = e->members[i];
-        int done = 0, j = 0;
-        while (done < nsteps) {
-            const int kk = nev > 0 ? std::min(sums_every, nsteps - done) : nsteps - done;
-            const bool rec = nev > 0 && kk == sums_every && j < nev;
-            int r = step_impl(h, kk, rec ? CB_STEP_SUMS : 0, false);
-            if (r != CB_OK) { err = cudaErrorLaunchFailure; break; }
-            if (rec) {
-                k_state_to_record<<<1, 32, 0, h->stream>>>(h->st, h->k.dxLD, drec + (size_t)i * nev + j);
-                ++j;
+        std::vector<double> t_start(count);
+        for (int i = 0; i < count; ++i) t_start[i] = e->members[i]->t;
+        cudaError_t err = cudaSuccess;
+        /* resident classes: one launch each, on their own streams */
+        for (auto &c : e->classes) {
+            std::vector<EnsMember> host(c.idx.size());
+            for (size_t q = 0; q < c.idx.size(); ++q) {
+                cb_handle *h = e->members[c.idx[q]];
+                flush_pending(h);
+                cudaStreamSynchronize(h->stream);
+                host[q].phi = h->phi[h->cphi];
+                host[q].pi = h->pi[h->cpi];
+                host[q].k = h->k;
+                host[q].out_index = c.idx[q] * nev;
+                int ex;
+                host[q].dx_pow2 = std::fabs(std::frexp(h->k.dx, &ex)) == 0.5 ? 1 : 0;
             }
-            done += kk;
+            err = cudaMemcpyAsync(c.dev, host.data(), host.size() * sizeof(EnsMember), cudaMemcpyHostToDevice, c.stream);
+            if (err == cudaSuccess)
+                err = launch_resident(c.prec, c.dev, (int)c.idx.size(), c.cs, c.threads, nsteps, sums_every, drec,
+                                      resident_smem(c.prec, c.n, c.cs), c.stream);
+            if (err != cudaSuccess) break;
         }
-    }
-    for (auto &c : e->classes) if (err == cudaSuccess) err = cudaStreamSynchronize(c.stream);
-    for (int i : e->own) if (err == cudaSuccess) err = cudaStreamSynchronize(e->members[i]->stream);
-    std::vector<EnsRecord> rec((size_t)count * nev);
-    if (err == cudaSuccess && nev > 0)
-        err = cudaMemcpy(rec.data(), drec, rec.size() * sizeof(EnsRecord), cudaMemcpyDeviceToHost);
-    cudaFree(drec);
-    if (err != cudaSuccess) return cuda_fail(nullptr, err, "cb_ensemble_step");
-    /* lines of the resident members (static background: a = 1, H = C = 0) and times */
-    for (int i = 0; i < count; ++i) {
-        cb_handle *h = e->members[i];
-        const bool own = std::find(e->own.begin(), e->own.end(), i) != e->own.end();
-        double t = t_start[i];
-        int stepped = 0;
-        for (int j = 0; j < nev; ++j) {
-            for (; stepped < (j + 1) * sums_every; ++stepped) t += h->p.dt;
-            cb_sums &o = out[(size_t)i * nev + j];
-            const EnsRecord &r = rec[(size_t)i * nev + j];
-            std::memset(&o, 0, sizeof o);
-            o.t = t;
-            o.a = 1.0;
-            if (own || r.v[S_EKIN_IN] < 0) {
-                o.ekin = r.v[S_EK]; o.epot = r.v[S_EP]; o.egrad = r.v[S_EG];
+        /* the others: their own step kernels on their own streams, records copied on the device */
+        for (int i : e->own) {
+            if (err != cudaSuccess) break;
+            cb_handle *h = e->members[i];
+            int done = 0, j = 0;
+            while (done < nsteps) {
+                const int kk = nev > 0 ? std::min(sums_every, nsteps - done) : nsteps - done;
+                const bool rec = nev > 0 && kk == sums_every && j < nev;
+                int r = step_impl(h, kk, rec ? CB_STEP_SUMS : 0, false);
+                if (r != CB_OK) { err = cudaErrorLaunchFailure; break; }
+                if (rec) {
+                    k_state_to_record<<<1, 32, 0, h->stream>>>(h->st, h->k.dxLD, drec + (size_t)i * nev + j);
+                    ++j;
+                }
+                done += kk;
+            }
+        }
+        for (auto &c : e->classes) if (err == cudaSuccess) err = cudaStreamSynchronize(c.stream);
+        for (int i : e->own) if (err == cudaSuccess) err = cudaStreamSynchronize(e->members[i]->stream);
+        std::vector<EnsRecord> rec((size_t)count * nev);
+        if (err == cudaSuccess && nev > 0)
+            err = cudaMemcpy(rec.data(), drec, rec.size() * sizeof(EnsRecord), cudaMemcpyDeviceToHost);
+        cudaFree(drec);
+        if (err != cudaSuccess) return cuda_fail(nullptr, err, "cb_ensemble_step");
+        /* lines of the resident members (static background: a = 1, H = C = 0) and times */
+        for (int i = 0; i < count; ++i) {
+            cb_handle *h = e->members[i];
+            const bool own = std::find(e->own.begin(), e->own.end(), i) != e->own.end();
+            double t = t_start[i];
+            int stepped = 0;
+            for (int j = 0; j < nev; ++j) {
+                for (; stepped < (j + 1) * sums_every; ++stepped) t += h->p.dt;
+                cb_sums &o = out[(size_t)i * nev + j];
+                const EnsRecord &r = rec[(size_t)i * nev + j];
+                std::memset(&o, 0, sizeof o);
+                o.t = t;
+                o.a = 1.0;
+                if (own || r.v[S_EKIN_IN] < 0) {
+                    o.ekin = r.v[S_EK]; o.epot = r.v[S_EP]; o.egrad = r.v[S_EG];
+                    o.etot = o.ekin + o.epot + o.egrad;
+                    o.avphi = r.v[S_PHI]; o.avphip = r.v[S_V];
+                    o.ekin_var = r.v[Q_EK]; o.epot_var = r.v[Q_EP]; o.egrad_var = r.v[Q_EG]; o.etot_var = r.v[Q_ET];
+                    o.avphi_var = r.v[Q_PHI]; o.avphip_var = r.v[Q_V];
+                    continue;
+                }
+                /* the scalar part of measureEnergies for a = 1 (bubble.cpp:812-843) */
+                const double dxLD = h->k.dxLD, dxLD2 = dxLD * dxLD;
+                const double ekhalf = r.v[S_EK] * dxLD, ekprev = r.v[S_EKIN_IN] * dxLD;
+                o.ekin = 0.5 * (ekhalf + ekprev);
+                o.epot = r.v[S_EP] * dxLD;
+                o.egrad = r.v[S_EG] * dxLD;
                 o.etot = o.ekin + o.epot + o.egrad;
-                o.avphi = r.v[S_PHI]; o.avphip = r.v[S_V];
-                o.ekin_var = r.v[Q_EK]; o.epot_var = r.v[Q_EP]; o.egrad_var = r.v[Q_EG]; o.etot_var = r.v[Q_ET];
-                o.avphi_var = r.v[Q_PHI]; o.avphip_var = r.v[Q_V];
-                continue;
+                o.avphi = r.v[S_PHI] * dxLD;
+                o.avphip = r.v[S_V] * dxLD;
+                o.ekin_var = r.v[Q_EK] * dxLD2;
+                o.epot_var = r.v[Q_EP] * dxLD2;
+                o.egrad_var = r.v[Q_EG] * dxLD2;
+                o.etot_var = r.v[Q_ET] * dxLD2;
+                o.avphi_var = r.v[Q_PHI] * dxLD2;
+                o.avphip_var = r.v[Q_V] * dxLD2;
+                o.ekin_half_prev = ekhalf;
             }
-            /* the scalar part of measureEnergies for a = 1 (bubble.cpp:812-843) */
-            const double dxLD = h->k.dxLD, dxLD2 = dxLD * dxLD;
-            const double ekhalf = r.v[S_EK] * dxLD, ekprev = r.v[S_EKIN_IN] * dxLD;
-            o.ekin = 0.5 * (ekhalf + ekprev);
-            o.epot = r.v[S_EP] * dxLD;
-            o.egrad = r.v[S_EG] * dxLD;
-            o.etot = o.ekin + o.epot + o.egrad;
-            o.avphi = r.v[S_PHI] * dxLD;
-            o.avphip = r.v[S_V] * dxLD;
-            o.ekin_var = r.v[Q_EK] * dxLD2;
-            o.epot_var = r.v[Q_EP] * dxLD2;
-            o.egrad_var = r.v[Q_EG] * dxLD2;
-            o.etot_var = r.v[Q_ET] * dxLD2;
-            o.avphi_var = r.v[Q_PHI] * dxLD2;
-            o.avphip_var = r.v[Q_V] * dxLD2;
-            o.ekin_half_prev = ekhalf;
+            if (!own) {
+                for (; stepped < nsteps; ++stepped) t += h->p.dt;
+                h->t = t;
+                h->steps_done += nsteps;
+            }
         }
-        if (!own) {
-            for (; stepped < nsteps; ++stepped) t += h->p.dt;
-            h->t = t;
-            h->steps_done += nsteps;
-        }
-    }
-    return CB_OK;
+        return CB_OK;
+    });
 }
 
 }  // extern "C"

@@ -619,31 +619,33 @@ cudaError_t fft_bins(FftState *f, double L, cudaStream_t s) {
 using namespace cb;
 
 extern "C" int cb_power_spectrum(cb_handle *h, double *power, double *weight, double *ksum, int nbins) {
-    if (!h) return fail(nullptr, CB_EINVAL, "handle is NULL");
-    const int nb = (int)(std::sqrt(double(h->p.d)) * h->p.n_grids / 2) + 1;
-    if (nbins != nb) return fail(h, CB_EINVAL, "nbins must equal cb_nbins(d, n_grids)");
-    if (!power || !weight || !ksum) return fail(h, CB_EINVAL, "output pointers must not be NULL");
-    int r = flush_pending(h);
-    if (r != CB_OK) return r;
-    if (!h->fft) {
-        FftState *f = nullptr;
-        if ((r = fft_setup(h, f, h->p.d, h->p.n_grids, h->stream)) != CB_OK) return r;
-        h->fft = f;
-    }
-    cudaError_t e = fft_r2c(h->fft, h->prec, h->phi[h->cphi], h->stream);
-    if (e == cudaSuccess) e = fft_bins(h->fft, h->p.L, h->stream);
-    std::vector<double> host(3 * (size_t)nb);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(host.data(), h->fft->bins_out, host.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                            h->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) return cuda_fail(h, e, "power spectrum");
-    for (int b = 0; b < nb; ++b) {
-        power[b] = host[b];
-        weight[b] = host[nb + b];
-        ksum[b] = host[2 * nb + b];
-    }
-    return CB_OK;
+    return cb::guard(h, [&]() -> int {
+        if (!h) return fail(nullptr, CB_EINVAL, "handle is NULL");
+        const int nb = (int)(std::sqrt(double(h->p.d)) * h->p.n_grids / 2) + 1;
+        if (nbins != nb) return fail(h, CB_EINVAL, "nbins must equal cb_nbins(d, n_grids)");
+        if (!power || !weight || !ksum) return fail(h, CB_EINVAL, "output pointers must not be NULL");
+        int r = flush_pending(h);
+        if (r != CB_OK) return r;
+        if (!h->fft) {
+            FftState *f = nullptr;
+            if ((r = fft_setup(h, f, h->p.d, h->p.n_grids, h->stream)) != CB_OK) return r;
+            h->fft = f;
+        }
+        cudaError_t e = fft_r2c(h->fft, h->prec, h->phi[h->cphi], h->stream);
+        if (e == cudaSuccess) e = fft_bins(h->fft, h->p.L, h->stream);
+        std::vector<double> host(3 * (size_t)nb);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(host.data(), h->fft->bins_out, host.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return cuda_fail(h, e, "power spectrum");
+        for (int b = 0; b < nb; ++b) {
+            power[b] = host[b];
+            weight[b] = host[nb + b];
+            ksum[b] = host[2 * nb + b];
+        }
+        return CB_OK;
+    });
 }
 
 namespace cb {
@@ -665,53 +667,57 @@ int device_c2r(int d, int n, const double *half_host, double *out_dev, cudaStrea
 /* Standalone c2r (host half-complex in, host real out); used by the thermal
  * initial condition and for checking the inverse DFT. */
 extern "C" int cb_dft_c2r(int d, int n, const double *in, double *out) {
-    if (d < 1 || d > 3 || n < 2 || !in || !out) return fail(nullptr, CB_EINVAL, "bad arguments to cb_dft_c2r");
-    size_t N = 1;
-    for (int i = 0; i < d; ++i) N *= (size_t)n;
-    cudaStream_t s;
-    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return cuda_fail(nullptr, e, "creating a stream");
-    FftState *f = nullptr;
-    int r = fft_setup(nullptr, f, d, n, s);
-    if (r != CB_OK) { cudaStreamDestroy(s); return r; }
-    double *dev = nullptr;
-    e = cudaMalloc(&dev, N * sizeof(double));
-    if (e == cudaSuccess) e = cudaMemcpyAsync(f->half, in, f->half_elems * sizeof(double2), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = fft_c2r(f, dev, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dev, N * sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(dev);
-    cudaFreeAsync(f->tw, s); cudaFreeAsync(f->half, s); cudaFreeAsync(f->hist, s); cudaFreeAsync(f->bins_out, s);
-    cudaStreamSynchronize(s);
-    delete f;
-    cudaStreamDestroy(s);
-    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cb_dft_c2r");
-    return CB_OK;
+    return cb::guard(nullptr, [&]() -> int {
+        if (d < 1 || d > 3 || n < 2 || !in || !out) return fail(nullptr, CB_EINVAL, "bad arguments to cb_dft_c2r");
+        size_t N = 1;
+        for (int i = 0; i < d; ++i) N *= (size_t)n;
+        cudaStream_t s;
+        cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(nullptr, e, "creating a stream");
+        FftState *f = nullptr;
+        int r = fft_setup(nullptr, f, d, n, s);
+        if (r != CB_OK) { cudaStreamDestroy(s); return r; }
+        double *dev = nullptr;
+        e = cudaMalloc(&dev, N * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemcpyAsync(f->half, in, f->half_elems * sizeof(double2), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = fft_c2r(f, dev, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out, dev, N * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        cudaFree(dev);
+        cudaFreeAsync(f->tw, s); cudaFreeAsync(f->half, s); cudaFreeAsync(f->hist, s); cudaFreeAsync(f->bins_out, s);
+        cudaStreamSynchronize(s);
+        delete f;
+        cudaStreamDestroy(s);
+        if (e != cudaSuccess) return cuda_fail(nullptr, e, "cb_dft_c2r");
+        return CB_OK;
+    });
 }
 
 /* Standalone r2c (host in, host out) for checking the DFT itself. */
 extern "C" int cb_dft_r2c(int d, int n, const double *in, double *out) {
-    if (d < 1 || d > 3 || n < 2 || !in || !out) return fail(nullptr, CB_EINVAL, "bad arguments to cb_dft_r2c");
-    size_t N = 1;
-    for (int i = 0; i < d; ++i) N *= (size_t)n;
-    cudaStream_t s;
-    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return cuda_fail(nullptr, e, "creating a stream");
-    FftState *f = nullptr;
-    int r = fft_setup(nullptr, f, d, n, s);
-    if (r != CB_OK) { cudaStreamDestroy(s); return r; }
-    double *dev = nullptr;
-    e = cudaMalloc(&dev, N * sizeof(double));
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dev, in, N * sizeof(double), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = fft_r2c(f, P_FP64, dev, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(out, f->half, f->half_elems * sizeof(double2), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(dev);
-    cudaFreeAsync(f->tw, s); cudaFreeAsync(f->half, s); cudaFreeAsync(f->hist, s); cudaFreeAsync(f->bins_out, s);
-    cudaStreamSynchronize(s);
-    delete f;
-    cudaStreamDestroy(s);
-    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cb_dft_r2c");
-    return CB_OK;
+    return cb::guard(nullptr, [&]() -> int {
+        if (d < 1 || d > 3 || n < 2 || !in || !out) return fail(nullptr, CB_EINVAL, "bad arguments to cb_dft_r2c");
+        size_t N = 1;
+        for (int i = 0; i < d; ++i) N *= (size_t)n;
+        cudaStream_t s;
+        cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(nullptr, e, "creating a stream");
+        FftState *f = nullptr;
+        int r = fft_setup(nullptr, f, d, n, s);
+        if (r != CB_OK) { cudaStreamDestroy(s); return r; }
+        double *dev = nullptr;
+        e = cudaMalloc(&dev, N * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dev, in, N * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = fft_r2c(f, P_FP64, dev, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(out, f->half, f->half_elems * sizeof(double2), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        cudaFree(dev);
+        cudaFreeAsync(f->tw, s); cudaFreeAsync(f->half, s); cudaFreeAsync(f->hist, s); cudaFreeAsync(f->bins_out, s);
+        cudaStreamSynchronize(s);
+        delete f;
+        cudaStreamDestroy(s);
+        if (e != cudaSuccess) return cuda_fail(nullptr, e, "cb_dft_r2c");
+        return CB_OK;
+    });
 }

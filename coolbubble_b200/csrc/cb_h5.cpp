@@ -562,65 +562,71 @@ extern "C" {
 int cb_h5_write_floats(const char *path, int rank, const int64_t *dims, const int64_t *chunk, int nsets,
                        const char *const *names, const float *const *data, int nattrs,
                        const char *const *attr_names, const double *attr_values, int deflate_level, int threads) {
-    if (!path || !dims || !chunk) return fail(nullptr, CB_EINVAL, "path, dims and chunk must not be NULL");
-    if (rank < 1 || rank > 3) return fail(nullptr, CB_EINVAL, "rank must be 1, 2 or 3");
-    if (nsets < 0 || nsets > MAX_SETS) return fail(nullptr, CB_EINVAL, "between 0 and 8 datasets");
-    if (nattrs < 0 || (nattrs && (!attr_names || !attr_values)))
-        return fail(nullptr, CB_EINVAL, "attribute names and values must not be NULL");
-    if (nsets && (!names || !data)) return fail(nullptr, CB_EINVAL, "dataset names and data must not be NULL");
-    if (deflate_level < 0 || deflate_level > 9) return fail(nullptr, CB_EINVAL, "deflate level must be 0..9");
-    Geometry g{};
-    g.rank = rank;
-    g.total = 1;
-    g.chunk_elems = 1;
-    for (int a = 0; a < rank; ++a) {
-        if (dims[a] < 1 || chunk[a] < 1 || chunk[a] > dims[a])
-            return fail(nullptr, CB_EINVAL, "dims must be >= 1 and 1 <= chunk <= dims");
-        g.dims[a] = (uint64_t)dims[a];
-        g.chunk[a] = (uint64_t)chunk[a];
-        g.nchunk[a] = (g.dims[a] + g.chunk[a] - 1) / g.chunk[a];
-        g.total *= g.nchunk[a];
-        g.chunk_elems *= (size_t)g.chunk[a];
-    }
-    if (g.chunk_elems * sizeof(float) >= (size_t(1) << 32)) return fail(nullptr, CB_EINVAL, "chunk of 4 GiB or more");
-    for (int s = 0; s < nsets; ++s)
-        if (!names[s] || !names[s][0] || !data[s]) return fail(nullptr, CB_EINVAL, "empty dataset name or NULL data");
-    for (int i = 0; i < nattrs; ++i)
-        if (!attr_names[i] || !attr_names[i][0]) return fail(nullptr, CB_EINVAL, "empty attribute name");
-    std::string why;
-    const int r = write_file(path, g, nsets, names, data, nattrs, attr_names, attr_values, deflate_level, threads, why);
-    if (r != CB_OK) return fail(nullptr, r, why);
-    return CB_OK;
+    return cb::guard(nullptr, [&]() -> int {
+        if (!path || !dims || !chunk) return fail(nullptr, CB_EINVAL, "path, dims and chunk must not be NULL");
+        if (rank < 1 || rank > 3) return fail(nullptr, CB_EINVAL, "rank must be 1, 2 or 3");
+        if (nsets < 0 || nsets > MAX_SETS) return fail(nullptr, CB_EINVAL, "between 0 and 8 datasets");
+        if (nattrs < 0 || (nattrs && (!attr_names || !attr_values)))
+            return fail(nullptr, CB_EINVAL, "attribute names and values must not be NULL");
+        if (nsets && (!names || !data)) return fail(nullptr, CB_EINVAL, "dataset names and data must not be NULL");
+        if (deflate_level < 0 || deflate_level > 9) return fail(nullptr, CB_EINVAL, "deflate level must be 0..9");
+        Geometry g{};
+        g.rank = rank;
+        g.total = 1;
+        g.chunk_elems = 1;
+        for (int a = 0; a < rank; ++a) {
+            if (dims[a] < 1 || chunk[a] < 1 || chunk[a] > dims[a])
+                return fail(nullptr, CB_EINVAL, "dims must be >= 1 and 1 <= chunk <= dims");
+            g.dims[a] = (uint64_t)dims[a];
+            g.chunk[a] = (uint64_t)chunk[a];
+            g.nchunk[a] = (g.dims[a] + g.chunk[a] - 1) / g.chunk[a];
+            g.total *= g.nchunk[a];
+            g.chunk_elems *= (size_t)g.chunk[a];
+        }
+        if (g.chunk_elems * sizeof(float) >= (size_t(1) << 32)) return fail(nullptr, CB_EINVAL, "chunk of 4 GiB or more");
+        for (int s = 0; s < nsets; ++s)
+            if (!names[s] || !names[s][0] || !data[s]) return fail(nullptr, CB_EINVAL, "empty dataset name or NULL data");
+        for (int i = 0; i < nattrs; ++i)
+            if (!attr_names[i] || !attr_names[i][0]) return fail(nullptr, CB_EINVAL, "empty attribute name");
+        std::string why;
+        const int r = write_file(path, g, nsets, names, data, nattrs, attr_names, attr_values, deflate_level, threads, why);
+        if (r != CB_OK) return fail(nullptr, r, why);
+        return CB_OK;
+    });
 }
 
 int cb_out_field(cb_handle *h, const char *path, int threads) {
-    if (!h || !path) return fail(h, CB_EINVAL, "handle and path must not be NULL");
-    if (h->writer) return fail(h, CB_EBUSY, "a snapshot write is in flight (cb_out_field_wait first)");
-    cb::Snapshot snap;
-    int r = prepare_snapshot(h, path, threads, snap);
-    if (r != CB_OK) return r;
-    std::string err;
-    r = write_snapshot(snap, err);
-    return r == CB_OK ? CB_OK : fail(h, r, err);
+    return cb::guard(h, [&]() -> int {
+        if (!h || !path) return fail(h, CB_EINVAL, "handle and path must not be NULL");
+        if (h->writer) return fail(h, CB_EBUSY, "a snapshot write is in flight (cb_out_field_wait first)");
+        cb::Snapshot snap;
+        int r = prepare_snapshot(h, path, threads, snap);
+        if (r != CB_OK) return r;
+        std::string err;
+        r = write_snapshot(snap, err);
+        return r == CB_OK ? CB_OK : fail(h, r, err);
+    });
 }
 
 int cb_out_field_async(cb_handle *h, const char *path, int threads) {
-    if (!h || !path) return fail(h, CB_EINVAL, "handle and path must not be NULL");
-    if (h->writer) return fail(h, CB_EBUSY, "a snapshot write is in flight (cb_out_field_wait first)");
-    auto snap = std::make_shared<cb::Snapshot>();
-    /* leave one host thread to the caller, who keeps launching steps */
-    if (threads <= 0) threads = std::max(1, omp_get_max_threads() - 1);
-    int r = prepare_snapshot(h, path, threads, *snap);
-    if (r != CB_OK) return r;
-    auto *w = new cb::SnapshotWriter;
-    try {
-        w->th = std::thread([w, snap] { w->status = write_snapshot(*snap, w->err); });
-    } catch (...) {
-        delete w;
-        return fail(h, CB_ENOMEM, "cannot start the snapshot writer thread");
-    }
-    h->writer = w;
-    return CB_OK;
+    return cb::guard(h, [&]() -> int {
+        if (!h || !path) return fail(h, CB_EINVAL, "handle and path must not be NULL");
+        if (h->writer) return fail(h, CB_EBUSY, "a snapshot write is in flight (cb_out_field_wait first)");
+        auto snap = std::make_shared<cb::Snapshot>();
+        /* leave one host thread to the caller, who keeps launching steps */
+        if (threads <= 0) threads = std::max(1, omp_get_max_threads() - 1);
+        int r = prepare_snapshot(h, path, threads, *snap);
+        if (r != CB_OK) return r;
+        auto *w = new cb::SnapshotWriter;
+        try {
+            w->th = std::thread([w, snap] { w->status = write_snapshot(*snap, w->err); });
+        } catch (...) {
+            delete w;
+            return fail(h, CB_ENOMEM, "cannot start the snapshot writer thread");
+        }
+        h->writer = w;
+        return CB_OK;
+    });
 }
 
 int cb_out_field_wait(cb_handle *h) {

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <new>
+#include <stdexcept>
 #include <string>
 #include <thread>
 #include <vector>
@@ -62,6 +64,20 @@ struct cb_handle {
 
 namespace cb {
 int fail(cb_handle *h, int status, const std::string &msg);
+/* Runs the body of an ABI entry point that allocates host memory: nothing
+ * throws across the C ABI, a failed allocation becomes CB_ENOMEM. */
+template <class F>
+int guard(cb_handle *h, F &&body) noexcept {
+    try {
+        return body();
+    } catch (const std::bad_alloc &) {
+        return fail(h, -2 /* CB_ENOMEM */, "host memory allocation failed");
+    } catch (const std::exception &ex) {
+        return fail(h, -1 /* CB_EINVAL */, ex.what());
+    } catch (...) {
+        return fail(h, -1 /* CB_EINVAL */, "unexpected exception");
+    }
+}
 int cuda_fail(cb_handle *h, cudaError_t e, const char *what);
 int sync(cb_handle *h, const char *what);
 int flush_pending(cb_handle *h);

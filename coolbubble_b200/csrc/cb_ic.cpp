@@ -230,95 +230,97 @@ int parse_positions(const char *text, std::vector<double> &xyz) { return read_po
 
 extern "C" int cb_initial_condition(const cb_params *p, const cb_ic_params *ic, const char *xns_in, double *phi0,
                                     double *pi0, char *xns_out, size_t xns_cap, size_t *xns_len) {
-    if (!p || !ic || !phi0 || !pi0) return cb::fail(nullptr, CB_EINVAL, "p, ic, phi0 and pi0 must not be NULL");
-    if (p->d < 1 || p->d > 3 || p->n_grids < 2 || !(p->L > 0))
-        return cb::fail(nullptr, CB_EINVAL, "bad lattice parameters");
-    const int d = p->d, n = p->n_grids;
-    const double L = p->L, c = p->c;
-    size_t N = 1;
-    for (int i = 0; i < d; ++i) N *= (size_t)n;
-    if (xns_len) *xns_len = 0;
-    for (size_t i = 0; i < N; ++i) { phi0[i] = 0.0; pi0[i] = 0.0; }
-    const Fits f = fits(c, d);
-    if (d == 1) {
-        /* bubble.cpp:324-335: a bubble centred on the box edge (profiles around x = 0 and x = L) */
-        for (int i = 0; i < n; ++i) {
-            double x[3];
-            coords((size_t)i, 1, n, L, x);
-            double xx = x[0];
-            phi0[i] = std::min(phi0[i] + profile(xx * xx, f), f.phic);
-            xx = x[0] - L;
-            phi0[i] = std::min(phi0[i] + profile(xx * xx, f), f.phic);
-        }
-        return CB_OK;
-    }
-    if (ic->test == 1) {
-        /* bubble.cpp:338-353: a small sine wave around the true vacuum */
-        const double phi_true = 1.;
-        const double k = 2.0 * M_PI / (L / 40.0);
-        const double amp = 0.01 * phi_true;
-#pragma omp parallel for schedule(static)
-        for (long long si = 0; si < (long long)N; ++si) {
-            double x[3];
-            coords((size_t)si, d, n, L, x);
-            double w = 0.0;
-            for (int a = 0; a < d; ++a) w += amp * std::sin(k * x[a]);
-            phi0[si] = phi_true + w / double(d);
-        }
-        return CB_OK;
-    }
-    switch (ic->mode) {
-        case -2: {   /* bubble.cpp:356-369 */
-#pragma omp parallel for schedule(static)
-            for (long long si = 0; si < (long long)N; ++si) {
+    return cb::guard(nullptr, [&]() -> int {
+        if (!p || !ic || !phi0 || !pi0) return cb::fail(nullptr, CB_EINVAL, "p, ic, phi0 and pi0 must not be NULL");
+        if (p->d < 1 || p->d > 3 || p->n_grids < 2 || !(p->L > 0))
+            return cb::fail(nullptr, CB_EINVAL, "bad lattice parameters");
+        const int d = p->d, n = p->n_grids;
+        const double L = p->L, c = p->c;
+        size_t N = 1;
+        for (int i = 0; i < d; ++i) N *= (size_t)n;
+        if (xns_len) *xns_len = 0;
+        for (size_t i = 0; i < N; ++i) { phi0[i] = 0.0; pi0[i] = 0.0; }
+        const Fits f = fits(c, d);
+        if (d == 1) {
+            /* bubble.cpp:324-335: a bubble centred on the box edge (profiles around x = 0 and x = L) */
+            for (int i = 0; i < n; ++i) {
                 double x[3];
-                coords((size_t)si, d, n, L, x);
-                const double a0 = x[0] - L / 2., a1 = x[1] - L / 2., a2 = x[2] - L / 2.;
-                const double r2 = d == 2 ? a0 * a0 + a1 * a1 : a0 * a0 + a1 * a1 + a2 * a2;
-                phi0[si] = std::min(phi0[si] + profile(r2, f), f.phic);
+                coords((size_t)i, 1, n, L, x);
+                double xx = x[0];
+                phi0[i] = std::min(phi0[i] + profile(xx * xx, f), f.phic);
+                xx = x[0] - L;
+                phi0[i] = std::min(phi0[i] + profile(xx * xx, f), f.phic);
             }
             return CB_OK;
         }
-        case -1: {   /* bubble.cpp:373-393 */
-            const double dr = ic->deltar;
-#pragma omp parallel for schedule(static)
+        if (ic->test == 1) {
+            /* bubble.cpp:338-353: a small sine wave around the true vacuum */
+            const double phi_true = 1.;
+            const double k = 2.0 * M_PI / (L / 40.0);
+            const double amp = 0.01 * phi_true;
+    #pragma omp parallel for schedule(static)
             for (long long si = 0; si < (long long)N; ++si) {
                 double x[3];
                 coords((size_t)si, d, n, L, x);
-                const double b0 = x[0] - L / 4 - dr, b1 = x[1] - L / 4. - dr, b2 = x[2] - L / 2.;
-                const double e0 = x[0] - 3. * L / 4. + dr, e1 = x[1] - 3. * L / 4 + dr, e2 = x[2] - L / 2.;
-                const double r1 = d == 2 ? b0 * b0 + b1 * b1 : b0 * b0 + b1 * b1 + b2 * b2;
-                const double r2 = d == 2 ? e0 * e0 + e1 * e1 : e0 * e0 + e1 * e1 + e2 * e2;
-                phi0[si] = std::min(phi0[si] + profile(r1, f), f.phic);
-                phi0[si] = std::min(phi0[si] + profile(r2, f), f.phic);
+                double w = 0.0;
+                for (int a = 0; a < d; ++a) w += amp * std::sin(k * x[a]);
+                phi0[si] = phi_true + w / double(d);
             }
             return CB_OK;
         }
-        case 1:
-        case 0: {
-            std::string text;
-            if (ic->mode == 1) {
-                text = random_positions(d, L, ic->n_bubbles, ic->position_seed, f);
-                if (xns_len) *xns_len = text.size();
-                if (xns_out) {
-                    if (xns_cap < text.size() + 1) return cb::fail(nullptr, CB_EINVAL, "xns_out buffer too small");
-                    std::memcpy(xns_out, text.c_str(), text.size() + 1);
+        switch (ic->mode) {
+            case -2: {   /* bubble.cpp:356-369 */
+    #pragma omp parallel for schedule(static)
+                for (long long si = 0; si < (long long)N; ++si) {
+                    double x[3];
+                    coords((size_t)si, d, n, L, x);
+                    const double a0 = x[0] - L / 2., a1 = x[1] - L / 2., a2 = x[2] - L / 2.;
+                    const double r2 = d == 2 ? a0 * a0 + a1 * a1 : a0 * a0 + a1 * a1 + a2 * a2;
+                    phi0[si] = std::min(phi0[si] + profile(r2, f), f.phic);
                 }
-            } else {
-                if (!xns_in) return cb::fail(nullptr, CB_EINVAL, "mode 0 needs the positions text (xns_in)");
-                text = xns_in;
+                return CB_OK;
             }
-            add_bubbles_from_text(text.c_str(), d, n, L, f, phi0, N);
-            return CB_OK;
+            case -1: {   /* bubble.cpp:373-393 */
+                const double dr = ic->deltar;
+    #pragma omp parallel for schedule(static)
+                for (long long si = 0; si < (long long)N; ++si) {
+                    double x[3];
+                    coords((size_t)si, d, n, L, x);
+                    const double b0 = x[0] - L / 4 - dr, b1 = x[1] - L / 4. - dr, b2 = x[2] - L / 2.;
+                    const double e0 = x[0] - 3. * L / 4. + dr, e1 = x[1] - 3. * L / 4 + dr, e2 = x[2] - L / 2.;
+                    const double r1 = d == 2 ? b0 * b0 + b1 * b1 : b0 * b0 + b1 * b1 + b2 * b2;
+                    const double r2 = d == 2 ? e0 * e0 + e1 * e1 : e0 * e0 + e1 * e1 + e2 * e2;
+                    phi0[si] = std::min(phi0[si] + profile(r1, f), f.phic);
+                    phi0[si] = std::min(phi0[si] + profile(r2, f), f.phic);
+                }
+                return CB_OK;
+            }
+            case 1:
+            case 0: {
+                std::string text;
+                if (ic->mode == 1) {
+                    text = random_positions(d, L, ic->n_bubbles, ic->position_seed, f);
+                    if (xns_len) *xns_len = text.size();
+                    if (xns_out) {
+                        if (xns_cap < text.size() + 1) return cb::fail(nullptr, CB_EINVAL, "xns_out buffer too small");
+                        std::memcpy(xns_out, text.c_str(), text.size() + 1);
+                    }
+                } else {
+                    if (!xns_in) return cb::fail(nullptr, CB_EINVAL, "mode 0 needs the positions text (xns_in)");
+                    text = xns_in;
+                }
+                add_bubbles_from_text(text.c_str(), d, n, L, f, phi0, N);
+                return CB_OK;
+            }
+            case -3: {   /* bubble.cpp:219-228 */
+                const double mT = std::sqrt(2 * (c + 6));
+                const double T = ic->trad * mT;
+                const double mF = std::sqrt(2 * c);
+                int st = thermal_field(d, n, L, T, mF, false, ic->thermal_seed, "thermalspec", phi0);
+                if (st == CB_OK) st = thermal_field(d, n, L, T, mF, true, ic->thermal_seed, "velocitythermalspec", pi0);
+                return st;
+            }
         }
-        case -3: {   /* bubble.cpp:219-228 */
-            const double mT = std::sqrt(2 * (c + 6));
-            const double T = ic->trad * mT;
-            const double mF = std::sqrt(2 * c);
-            int st = thermal_field(d, n, L, T, mF, false, ic->thermal_seed, "thermalspec", phi0);
-            if (st == CB_OK) st = thermal_field(d, n, L, T, mF, true, ic->thermal_seed, "velocitythermalspec", pi0);
-            return st;
-        }
-    }
-    return cb::fail(nullptr, CB_EINVAL, "mode must be between -3 and 1");
+        return cb::fail(nullptr, CB_EINVAL, "mode must be between -3 and 1");
+    });
 }

@@ -180,23 +180,25 @@ using namespace cb;
 
 extern "C" int cb_create_from_seed(const cb_params *p, const cb_ic_params *ic, const char *xns_in, cb_sums *initial,
                                    char *xns_out, size_t xns_cap, size_t *xns_len, cb_handle **out) {
-    if (!ic || !out) return fail(nullptr, CB_EINVAL, "ic and out must not be NULL");
-    cb_handle *h = nullptr;
-    int r = alloc_handle(p, &h);
-    if (r != CB_OK) return r;
-    std::string text;
-    r = device_initial_condition(h, ic, xns_in, &text);
-    if (r == CB_OK) {
-        if (xns_len) *xns_len = text.size();
-        if (xns_out && xns_cap < text.size() + 1) r = fail(h, CB_EINVAL, "xns_out buffer too small");
-        else if (xns_out) std::memcpy(xns_out, text.c_str(), text.size() + 1);
-    }
-    if (r == CB_OK) r = finish_create_from_device_ic(h, initial);
-    if (r != CB_OK) {
-        fail(nullptr, r, h->err);
-        destroy_handle(h);
-        return r;
-    }
-    *out = h;
-    return CB_OK;
+    return cb::guard(nullptr, [&]() -> int {
+        if (!ic || !out) return fail(nullptr, CB_EINVAL, "ic and out must not be NULL");
+        cb_handle *h = nullptr;
+        int r = alloc_handle(p, &h);
+        if (r != CB_OK) return r;
+        std::string text;
+        r = device_initial_condition(h, ic, xns_in, &text);
+        if (r == CB_OK) {
+            if (xns_len) *xns_len = text.size();
+            if (xns_out && xns_cap < text.size() + 1) r = fail(h, CB_EINVAL, "xns_out buffer too small");
+            else if (xns_out) std::memcpy(xns_out, text.c_str(), text.size() + 1);
+        }
+        if (r == CB_OK) r = finish_create_from_device_ic(h, initial);
+        if (r != CB_OK) {
+            fail(nullptr, r, h->err);
+            destroy_handle(h);
+            return r;
+        }
+        *out = h;
+        return CB_OK;
+    });
 }

@@ -260,3 +260,17 @@ def test_reference_reader_opens_the_snapshots(tmp_path, monkeypatch):
         assert info == {"t": 2.5, "a": 1.5, "reduc": float(reduc)}
         assert len(axes) == D
         np.testing.assert_allclose(axes[0], (np.arange(m) * reduc + 0.5) * 16.0 / n_grids, rtol=0, atol=0)
+
+
+def test_host_allocation_failure_is_a_status(tmp_path):
+    """Nothing throws across the C ABI: an index of 2^40 chunks cannot be
+    allocated, and the call returns CB_ENOMEM with a message instead of
+    ending the process (no data is read before the allocation)."""
+    a = np.zeros(4, np.float32)
+    names = (L.C.c_char_p * 1)(b"phi")
+    data = (L._fp * 1)(L.fptr(a))
+    dims, chunk = (L.C.c_int64 * 1)(1 << 40), (L.C.c_int64 * 1)(1)
+    st = L.lib.cb_h5_write_floats(str(tmp_path / "huge.h5").encode(), 1, dims, chunk, 1, names, data, 0, None, None,
+                                  9, 1)
+    assert st == L.CB_ENOMEM
+    assert b"allocation" in L.lib.cb_last_error(None)
