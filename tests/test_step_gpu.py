@@ -311,6 +311,25 @@ def test_fp64_tiled_static_matches_oracle():
         assert field_err(f[k], fo[k]) <= FIELD_TOL, k
 
 
+def test_fp64_strip_kernel_2d_matches_oracle():
+    """The d = 2 column-strip kernel (1024^2 and up) against the oracle in FP64:
+    fields and box averages after 3 x 20 steps, local arrays included."""
+    import coolbubble_b200 as cb
+    from oracle import bridge as B
+    d, n, L, c = 2, 1024, 64.0, 4.0
+    dt = 0.1 * L / n
+    phi0, pi0 = bubbles(d, n, L, c, 5, seed=21), smooth_noise(d, n, 0.05, seed=22)
+    s = cb.Bubble(cb.make_params(d, n, L, c, dt), phi0, pi0)
+    o = B.Oracle(d, n, L, c, dt, phi0, pi0)
+    for _ in range(3):
+        got = s.step(20, sums=True, local=True)
+        o.step(20)
+        check_sums(got, o.scalars(), n ** d)
+    f, fo = s.fields(), o.fields()
+    for k in ("phi", "pi", "ekin", "egrad", "epot"):
+        assert field_err(f[k], fo[k]) <= FIELD_TOL, k
+
+
 def test_device_error_word_stays_clear():
     """The bounded waits of the tiled kernel never fired during a normal run."""
     import coolbubble_b200 as cb
