@@ -88,10 +88,12 @@ cudaError_t launch_step(int prec, const StepConst &k, bool drift_first, int sums
 /* Number of blocks (and so of partial-sum slots) a step launch may use. */
 size_t step_blocks(const StepConst &k);
 
-/* d = 2 kernel marching column strips down the rows (cb_step2.cu): static
- * background, n a multiple of the vector width, lattices of at least
- * STEP2_MIN_SITES sites (below that the generic tile kernel). */
+/* d = 2 kernel marching column strips down the rows (cb_step2.cu), also run
+ * on the single row of d = 1: static background, n a multiple of the vector
+ * width, lattices of at least STEP2_MIN_SITES (d = 2) / STEP1_MIN_SITES
+ * (d = 1) sites; below that the generic tile kernel. */
 constexpr size_t STEP2_MIN_SITES = size_t(1) << 20;   /* below 1024^2 both are launch-bound; the tiles win at 128^2 */
+constexpr size_t STEP1_MIN_SITES = size_t(1) << 20;   /* d = 1: at 2^18 sites the tiles still win (4.5 vs 5.7 us) */
 bool step2_applies(const StepConst &k, int prec, bool drift_first);
 size_t step2_blocks(const StepConst &k);
 cudaError_t launch_step2(int prec, const StepConst &k, int sums, const void *phi_in, const void *pi_in,

@@ -438,7 +438,7 @@ size_t step_blocks(const StepConst &k) {
         unsigned g3;
         if (step3_geometry(k, prec, tj, ns, sm, g3)) b = std::max(b, step3_partial_rows(k, prec));
     }
-    if (k.d == 2) b = std::max(b, step2_blocks(k));
+    if (k.d <= 2) b = std::max(b, step2_blocks(k));
     return b;
 }
 

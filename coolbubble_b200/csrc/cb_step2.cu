@@ -1,5 +1,6 @@
 /* cb_step2.cu -- the d = 2 step (static background) as column strips marched
- * down the rows of axis 0 (bubble.cpp:716-743, 849-876 for D = 2).
+ * down the rows of axis 0 (bubble.cpp:716-743, 849-876 for D = 2); d = 1 is
+ * the same kernel on a single row.
  *
  * A thread owns W consecutive sites of a row (one 16-byte vector: 4 floats or
  * 2 doubles) and walks down a band of rows. The rows above and below are the
@@ -10,8 +11,8 @@
  * value from global memory. Per row, phi and pi are read once and written
  * once; a band's two halo rows are the only reads twice.
  *
- * The per-site arithmetic is the generic tile kernel's for d = 2, expression
- * for expression (cb_step.cu), so the fields are identical to it (FP64: the
+ * The per-site arithmetic is the generic tile kernel's for d = 1 and 2,
+ * expression for expression (cb_step.cu), so the fields are identical to it (FP64: the
  * reference's evaluation order). The sums are accumulated per thread along
  * its strip: a different, fixed order (deterministic for a lattice size).
  */
@@ -32,7 +33,7 @@ namespace {
 constexpr int NT2 = 256;
 constexpr int TARGET_BLOCKS = 148 * 8;   /* about eight blocks per SM */
 
-template <typename T, int SUMS>
+template <typename T, int D, int SUMS>
 __global__ void __launch_bounds__(NT2) k_step2(StepConst k, int rows_per_band, const T *__restrict__ phi_in,
                                                 const T *__restrict__ pi_in, T *__restrict__ phi_out,
                                                 T *__restrict__ pi_out, T *__restrict__ loc_ek,
@@ -69,9 +70,11 @@ __global__ void __launch_bounds__(NT2) k_step2(StepConst k, int rows_per_band, c
     auto ldv = [&](const T *p, int r) { return *reinterpret_cast<const VT *>(p + (size_t)r * nn + k0); };
 
     Acc<T> acc[NSUM];
-    VT fm = ldv(phi_in, (r0 - 1 + n) % n);
-    VT f0 = ldv(phi_in, r0);
-    VT fp = ldv(phi_in, (r0 + 1) % n);
+    VT f0 = ldv(phi_in, r0), fm = f0, fp = f0;   /* d = 1: one row, no neighbours across rows */
+    if constexpr (D == 2) {
+        fm = ldv(phi_in, (r0 - 1 + n) % n);
+        fp = ldv(phi_in, (r0 + 1) % n);
+    }
     VT p0 = ldv(pi_in, r0);
     T el = left_lane ? (T)0 : phi_in[(size_t)r0 * nn + kl];
     T er = right_lane ? (T)0 : phi_in[(size_t)r0 * nn + kr];
@@ -80,7 +83,7 @@ __global__ void __launch_bounds__(NT2) k_step2(StepConst k, int rows_per_band, c
         /* the next iteration's rows, loaded before this row is computed */
         VT fq = fp, pq = p0;
         T eln = (T)0, ern = (T)0;
-        const bool more = r + 1 < r1;
+        const bool more = D == 2 && r + 1 < r1;
         if (more) {
             fq = ldv(phi_in, (r + 2) % n);
             pq = ldv(pi_in, r + 1);
@@ -104,7 +107,7 @@ __global__ void __launch_bounds__(NT2) k_step2(StepConst k, int rows_per_band, c
             /* Laplacian, axes in the reference's order (bubble.cpp:731-736) */
             const T tj = A::add(A::sub(dn, two), up);
             const T tk = A::add(A::sub(rgt, two), lft);
-            const T lap = A::add(tj, tk);
+            const T lap = D == 2 ? A::add(tj, tk) : tk;
             const T flap = A::mul(fl, lap);
             const T force = A::sub(dx2_pow2 ? A::mul(flap, inv_dx2) : A::div(flap, dx2), A::mul(fv, dV<T>(k, cur)));
             const T pinew = A::add(pic, A::mul(dt, force));
@@ -113,7 +116,7 @@ __global__ void __launch_bounds__(NT2) k_step2(StepConst k, int rows_per_band, c
             if (SUMS == SUM_FULL) {
                 /* forward gradients in the reference's naming (bubble.cpp:788-801) */
                 const T gx = grad(A::sub(rgt, cur));
-                const T gy = grad(A::sub(dn, cur));
+                const T gy = D == 2 ? grad(A::sub(dn, cur)) : (T)0;
                 const T gz = (T)0;
                 const T eg = A::mul(half, A::add(A::add(A::sq(gx), A::sq(gy)), A::sq(gz)));
                 const T ep = Vpot<T>(k, cur);
@@ -169,11 +172,16 @@ __global__ void __launch_bounds__(NT2) k_step2(StepConst k, int rows_per_band, c
     }
 }
 
-/* strips of NT2 vectors across a row, bands of rows down axis 0 */
+/* strips of NT2 vectors across a row, bands of rows down axis 0 (d = 1: one row) */
 void step2_grid(const StepConst &k, int prec, unsigned &strips, unsigned &bands, int &rows_per_band) {
     const int W = prec == P_FP64 ? 2 : 4;
     const int nv = k.n / W;
     strips = (unsigned)((nv + NT2 - 1) / NT2);
+    if (k.d == 1) {
+        bands = 1;
+        rows_per_band = 1;
+        return;
+    }
     int b = std::max(1, std::min(k.n, TARGET_BLOCKS / (int)strips));
     rows_per_band = std::max(4, (k.n + b - 1) / b);
     bands = (unsigned)((k.n + rows_per_band - 1) / rows_per_band);
@@ -183,8 +191,9 @@ void step2_grid(const StepConst &k, int prec, unsigned &strips, unsigned &bands,
 
 bool step2_applies(const StepConst &k, int prec, bool drift_first) {
     const int W = prec == P_FP64 ? 2 : 4;
-    return k.d == 2 && !drift_first && !k.force_generic && k.n % W == 0 && k.n >= 2 * W &&
-           (size_t)k.n * k.n >= STEP2_MIN_SITES;
+    if (drift_first || k.force_generic || k.n % W != 0 || k.n < 2 * W) return false;
+    if (k.d == 1) return (size_t)k.n >= STEP1_MIN_SITES;
+    return k.d == 2 && (size_t)k.n * k.n >= STEP2_MIN_SITES;
 }
 
 size_t step2_blocks(const StepConst &k) {
@@ -205,9 +214,16 @@ cudaError_t launch_step2(int prec, const StepConst &k, int sums, const void *phi
     int rpb;
     step2_grid(k, prec, strips, bands, rpb);
     const dim3 g(strips, bands);
+    /* one statement per use: each expansion returns, for d = 1 or d = 2 */
 #define CB_LAUNCH2(T, SU)                                                                                          \
-    return launch_pdl(k_step2<T, SU>, g, dim3(NT2), 0, s, k, rpb, (const T *)phi_in, (const T *)pi_in,            \
-                      (T *)phi_out, (T *)pi_out, (T *)le, (T *)lg, (T *)lp, st, partials)
+    do {                                                                                                           \
+        if (k.d == 1)                                                                                              \
+            return launch_pdl(k_step2<T, 1, SU>, g, dim3(NT2), 0, s, k, rpb, (const T *)phi_in,                   \
+                              (const T *)pi_in, (T *)phi_out, (T *)pi_out, (T *)le, (T *)lg, (T *)lp, st,         \
+                              partials);                                                                           \
+        return launch_pdl(k_step2<T, 2, SU>, g, dim3(NT2), 0, s, k, rpb, (const T *)phi_in, (const T *)pi_in,     \
+                          (T *)phi_out, (T *)pi_out, (T *)le, (T *)lg, (T *)lp, st, partials);                    \
+    } while (0)
     if (prec == P_FP64) {
         if (sums == SUM_FULL) CB_LAUNCH2(double, SUM_FULL);
         CB_LAUNCH2(double, SUM_NONE);

@@ -234,17 +234,19 @@ def test_tiled_kernel_equals_generic_kernel_fp64(case, monkeypatch):
         np.testing.assert_array_equal(fa[key], fb[key])
 
 
-@pytest.mark.parametrize("n,prec", [(1024, "fp64"), (1028, "fp32c"), (2048, "fp32c"), (1032, "fp64"),
-                                    (1026, "fp64"), (4100, "fp32c")])
-def test_strip_kernel_equals_generic_kernel_2d(n, prec, monkeypatch):
-    """The d = 2 strip kernel (column strips marched down the rows; lattices of
-    1024^2 sites and more) does the generic kernel's per-site arithmetic op for
-    op: bit-identical fields and local energy arrays over measured and
-    unmeasured steps; the box sums differ only in their order. Sizes cover rows
-    ending inside a warp (one vector in the last strip) and inside a block,
-    odd vector counts, several strips and bands."""
+@pytest.mark.parametrize("d,n,prec", [(2, 1024, "fp64"), (2, 1028, "fp32c"), (2, 2048, "fp32c"), (2, 1032, "fp64"),
+                                      (2, 1026, "fp64"), (2, 4100, "fp32c"), (1, 1 << 20, "fp64"),
+                                      (1, (1 << 20) + 4, "fp32c"), (1, (1 << 20) + 2, "fp64")])
+def test_strip_kernel_equals_generic_kernel_2d(d, n, prec, monkeypatch):
+    """The strip kernel (column strips marched down the rows; d = 2 lattices of
+    1024^2 sites and more, d = 1 rows of 2^20 and more) does the generic
+    kernel's per-site arithmetic op for op: bit-identical fields and local
+    energy arrays over measured and unmeasured steps; the box sums differ only
+    in their order. Sizes cover rows ending inside a warp (one vector in the
+    last strip) and inside a block, odd vector counts, several strips and
+    bands."""
     import coolbubble_b200 as cb
-    d, L, c = 2, n / 8.0, 4.0
+    L, c = n / 8.0, 4.0
     p = cb.make_params(d, n, L, c, 0.1 * L / n, precision=prec)
     phi0 = bubbles(d, n, L, c, 6, seed=7)
     pi0 = smooth_noise(d, n, 0.02, seed=8)
