@@ -342,18 +342,23 @@ struct BinConst {
 __device__ __forceinline__ long long sidx(long long i, int n) { return (i <= n / 2) ? i : i - n; }
 
 /* Shell sums of bubble.cpp:680-701 per block: smem histograms, then one row
- * of partials per block. A warp takes a row of the half-complex array; each
- * lane a contiguous run of the row's columns, along which the shell index
- * only grows: the lane adds into registers while its shell stays the same and
- * into the shared histogram when it changes. */
+ * of partials per block. A warp takes a row of the half-complex array in
+ * chunks of 256 columns, loaded coalesced into shared memory; each lane then
+ * takes 8 consecutive columns of the chunk, along which the shell index only
+ * grows: it adds into registers while its shell stays the same and into the
+ * shared histogram when it changes. */
+constexpr int BIN_CHUNK = 256;   /* columns a warp stages at once (8 per lane) */
+
 __global__ void __launch_bounds__(FFT_T) k_bins(BinConst bc, const double2 *__restrict__ half, double *hist) {
     extern __shared__ double sh[];
+    /* a warp's chunk of its row, loaded coalesced; one pad slot per 8 values so
+     * that lanes reading 8 consecutive values (16-byte accesses) hit distinct banks */
+    __shared__ double2 stage[FFT_T / 32][BIN_CHUNK + BIN_CHUNK / 8];
     double *pw = sh, *ws = sh + bc.nbins, *ks = sh + 2 * bc.nbins;
     for (int i = threadIdx.x; i < 3 * bc.nbins; i += blockDim.x) sh[i] = 0.0;
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int seg = (bc.h + 31) / 32;
-    const int j0 = lane * seg, j1 = min(bc.h, j0 + seg);
+    double2 *buf = stage[warp];
     const unsigned rows = (unsigned)bc.rows;
     for (unsigned r = blockIdx.x * nwarps + warp; r < rows; r += gridDim.x * nwarps) {
         double n2rows = 0.0;
@@ -366,50 +371,53 @@ __global__ void __launch_bounds__(FFT_T) k_bins(BinConst bc, const double2 *__re
             n2rows = __dadd_rn(s0 * s0, s1 * s1);
         }
         const double2 *row = half + (size_t)r * bc.h;
-        int cur = -1;
-        bool past = false;   /* beyond the last shell: so are the rest of the row's columns */
-        double ap = 0.0, aw = 0.0, ak = 0.0;
-        for (int jc = j0; jc < j1; jc += 8) {
-            /* the lane's next 8 values, loaded before any is used */
-            double2 fv[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) fv[u] = jc + u < j1 ? __ldg(&row[jc + u]) : make_double2(0.0, 0.0);
+        for (int c0 = 0; c0 < bc.h; c0 += BIN_CHUNK) {
+            /* the shell index grows with the column: a chunk that starts beyond the
+             * last shell ends the row (the same for every lane of the warp) */
+            if ((int)sqrt(__dadd_rn(n2rows, (double)c0 * (double)c0)) >= bc.nbins) break;
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-            const int j = jc + u;
-            if (j >= j1) break;
-            const double nn = sqrt(__dadd_rn(n2rows, (double)j * (double)j));
-            const int b = (int)nn;
-            if (b >= bc.nbins) {               /* the shell index grows with j */
-                past = true;
-                break;
+                const int e = lane + 32 * u, j = c0 + e;
+                buf[e + (e >> 3)] = j < bc.h ? __ldg(&row[j]) : make_double2(0.0, 0.0);
             }
-            if (b != cur) {
-                if (cur >= 0) {
-                    atomicAdd(&pw[cur], ap);
-                    atomicAdd(&ws[cur], aw);
-                    atomicAdd(&ks[cur], ak);
+            __syncwarp();
+            /* the lane's 8 consecutive columns: add into registers while the shell
+             * stays the same, into the shared histogram when it changes */
+            int cur = -1;
+            double ap = 0.0, aw = 0.0, ak = 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = 8 * lane + u, j = c0 + e;
+                if (j >= bc.h) break;
+                const double nn = sqrt(__dadd_rn(n2rows, (double)j * (double)j));
+                const int b = (int)nn;
+                if (b >= bc.nbins) break;
+                if (b != cur) {
+                    if (cur >= 0) {
+                        atomicAdd(&pw[cur], ap);
+                        atomicAdd(&ws[cur], aw);
+                        atomicAdd(&ks[cur], ak);
+                    }
+                    cur = b;
+                    ap = aw = ak = 0.0;
                 }
-                cur = b;
-                ap = aw = ak = 0.0;
+                const double w = (j == 0 || j == bc.n / 2) ? 1.0 : 2.0;
+                const double2 f = buf[e + (e >> 3)];
+                const double kc = __dmul_rn(nn, bc.dk);
+                double kd = kc;
+                if (bc.d >= 2) kd = __dmul_rn(kd, kc);
+                if (bc.d == 3) kd = __dmul_rn(kd, kc);
+                const double mag = __dadd_rn(__dmul_rn(f.x, f.x), __dmul_rn(f.y, f.y));
+                ap = __dadd_rn(ap, __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(w, bc.pref), kd), bc.pnorm), mag));
+                aw = __dadd_rn(aw, w);
+                ak = __dadd_rn(ak, __dmul_rn(w, kc));
             }
-            const double w = (j == 0 || j == bc.n / 2) ? 1.0 : 2.0;
-            const double2 f = fv[u];
-            const double kc = __dmul_rn(nn, bc.dk);
-            double kd = kc;
-            if (bc.d >= 2) kd = __dmul_rn(kd, kc);
-            if (bc.d == 3) kd = __dmul_rn(kd, kc);
-            const double mag = __dadd_rn(__dmul_rn(f.x, f.x), __dmul_rn(f.y, f.y));
-            ap = __dadd_rn(ap, __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(w, bc.pref), kd), bc.pnorm), mag));
-            aw = __dadd_rn(aw, w);
-            ak = __dadd_rn(ak, __dmul_rn(w, kc));
+            if (cur >= 0) {
+                atomicAdd(&pw[cur], ap);
+                atomicAdd(&ws[cur], aw);
+                atomicAdd(&ks[cur], ak);
             }
-            if (past) break;
-        }
-        if (cur >= 0) {
-            atomicAdd(&pw[cur], ap);
-            atomicAdd(&ws[cur], aw);
-            atomicAdd(&ks[cur], ak);
+            __syncwarp();   /* the chunk is read before the next one overwrites it */
         }
     }
     __syncthreads();
