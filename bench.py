@@ -37,11 +37,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    # configs[2] of the benchmark set: the HBM-resident headline stencil
+    # the headline: a 512^3 static lattice, c = 2, thermal-like start (HBM-resident stencil)
     "thermal-d3-n512": dict(d=3, n=512, L=64.0, c=2.0, expansion=0, mpl=200.0, precision="fp32c"),
     # the same stencil at 256^3 (2 x 64 MiB fields), for profiler captures
     "thermal-d3-n256": dict(d=3, n=256, L=32.0, c=2.0, expansion=0, mpl=200.0, precision="fp32c"),
-    # expanding background, smaller lattice
+    # a 256^3 lattice with bubbles and the self-consistent expanding background
     "bubbles-d3-n256-expanding": dict(d=3, n=256, L=32.0, c=4.0, expansion=1, mpl=10.0, precision="fp32c"),
     # a large 2-D lattice (column-strip kernel), for profiler captures
     "plain-d2-n8192": dict(d=2, n=8192, L=1024.0, c=4.0, expansion=0, mpl=200.0, precision="fp32c"),
@@ -325,7 +325,7 @@ def ensemble_members(count, seed):
 
 
 def run_ensemble_bench(args):
-    """256 independent d = 2 lattices stepped together (FP32C), and the
+    """The ensemble: 256 independent d = 2 lattices stepped together (FP32C), and the
     same ensemble in plain FP64; value = total site-updates/s of the ensemble."""
     import coolbubble_b200 as cb
     from coolbubble_b200 import _lib as L

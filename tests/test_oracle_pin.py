@@ -41,9 +41,9 @@ def test_oracle_matches_golden(name):
         s = o.scalars()
         ref = dict(zip(SCAL, g["scalars"][it]))
         for k in SCAL:
-            if k == "C":   # H^2 - rho/(3 Mpl^2) cancels: judge it on the scale of H^2
+            if k == "C":   # H^2 - rho/(3 Mpl^2) cancels: compared on the scale of H^2
                 assert abs(s[k] - ref[k]) <= 1e-12 * max(ref["H"] ** 2, 1e-300), it
-            elif k in ("avphi", "avphiP"):   # signed sums: judge them on sum |x| <= sqrt(N * sum x^2)
+            elif k in ("avphi", "avphiP"):   # signed sums: compared on sum |x| <= sqrt(N * sum x^2)
                 scale = np.sqrt(o.N * ref[k + "Var"])
                 assert abs(s[k] - ref[k]) <= 1e-12 * max(scale, 1e-300), (it, k)
             else:

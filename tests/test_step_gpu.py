@@ -223,7 +223,7 @@ def test_tiled_kernel_equals_generic_kernel_fp64(case, monkeypatch):
     a = tiled.step(25, sums=True, local=True)
     b = generic.step(25, sums=True, local=True)
     for key in a:
-        # C = H^2 - a^(2 alpha) Etot / (3 Mpl^2) cancels: judged on the H^2 scale;
+        # C = H^2 - a^(2 alpha) Etot / (3 Mpl^2) cancels: compared on the H^2 scale;
         # signed sums (<phi>, <phidot>) on the scale of sqrt(N sum x^2), a bound on sum |x|
         scale = abs(b["H"]) ** 2 if key == "C" else abs(b[key])
         if key in ("avphi", "avphip"):
@@ -259,7 +259,7 @@ def test_strip_kernel_equals_generic_kernel_2d(d, n, prec, monkeypatch):
         b = generic.step(steps, sums=True, local=True)
         tol = 1e-13 if prec == "fp64" else 1e-5
         for key in a:
-            # C = H^2 - Etot / (3 Mpl^2) with H = 0 here: judged on the scale of its terms
+            # C = H^2 - Etot / (3 Mpl^2) with H = 0 here: compared on the scale of its terms
             scale = abs(b["H"]) ** 2 + abs(b["etot"]) / (3 * 200.0 ** 2) if key == "C" else abs(b[key])
             if key in ("avphi", "avphip"):
                 scale = max(scale, (n ** d * b[key + "_var"]) ** 0.5)
