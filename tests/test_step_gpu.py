@@ -234,19 +234,23 @@ def test_tiled_kernel_equals_generic_kernel_fp64(case, monkeypatch):
         np.testing.assert_array_equal(fa[key], fb[key])
 
 
-@pytest.mark.parametrize("d,n,prec", [(2, 1024, "fp64"), (2, 1028, "fp32c"), (2, 2048, "fp32c"), (2, 1032, "fp64"),
-                                      (2, 1026, "fp64"), (2, 4100, "fp32c"), (1, 1 << 20, "fp64"),
-                                      (1, (1 << 20) + 4, "fp32c"), (1, (1 << 20) + 2, "fp64")])
-def test_strip_kernel_equals_generic_kernel_2d(d, n, prec, monkeypatch):
+@pytest.mark.parametrize("d,n,prec,L", [(2, 1024, "fp64", None), (2, 1028, "fp32c", None), (2, 2048, "fp32c", None),
+                                        (2, 1032, "fp64", None), (2, 1026, "fp64", None), (2, 4100, "fp32c", None),
+                                        (1, 1 << 20, "fp64", None), (1, (1 << 20) + 4, "fp32c", None),
+                                        (1, (1 << 20) + 2, "fp64", None), (2, 1032, "fp64", 100.0),
+                                        (1, 1 << 20, "fp64", 100000.0)])
+def test_strip_kernel_equals_generic_kernel_2d(d, n, prec, L, monkeypatch):
     """The strip kernel (column strips marched down the rows; d = 2 lattices of
     1024^2 sites and more, d = 1 rows of 2^20 and more) does the generic
     kernel's per-site arithmetic op for op: bit-identical fields and local
     energy arrays over measured and unmeasured steps; the box sums differ only
     in their order. Sizes cover rows ending inside a warp (one vector in the
     last strip) and inside a block, odd vector counts, several strips and
-    bands."""
+    bands, and (L = 100, 1e5) spacings whose square is not a power of two, where
+    FP64 divides as the reference does."""
     import coolbubble_b200 as cb
-    L, c = n / 8.0, 4.0
+    L = n / 8.0 if L is None else L
+    c = 4.0
     p = cb.make_params(d, n, L, c, 0.1 * L / n, precision=prec)
     phi0 = bubbles(d, n, L, c, 6, seed=7)
     pi0 = smooth_noise(d, n, 0.02, seed=8)
