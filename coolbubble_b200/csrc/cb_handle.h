@@ -71,11 +71,11 @@ int guard(cb_handle *h, F &&body) noexcept {
     try {
         return body();
     } catch (const std::bad_alloc &) {
-        return fail(h, -2 /* CB_ENOMEM */, "host memory allocation failed");
+        return fail(h, CB_ENOMEM, "host memory allocation failed");
     } catch (const std::exception &ex) {
-        return fail(h, -1 /* CB_EINVAL */, ex.what());
+        return fail(h, CB_EINVAL, ex.what());
     } catch (...) {
-        return fail(h, -1 /* CB_EINVAL */, "unexpected exception");
+        return fail(h, CB_EINVAL, "unexpected exception");
     }
 }
 int cuda_fail(cb_handle *h, cudaError_t e, const char *what);
