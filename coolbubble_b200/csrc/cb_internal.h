@@ -81,6 +81,12 @@ struct StepConst {
 /* Kernel launchers (cb_step.cu). Each returns the cudaError_t of the launch. */
 enum Prec { P_FP64 = 0, P_FP32 = 1 };
 
+/* Which sums a step kernel accumulates (the `sums` argument of the launchers).
+ * SUM_FRIEDMANN_EG: the Friedmann sums with the gradient energy (conformal
+ * time, alpha = 1); the staged d = 3 kernel takes it as its own variant so
+ * the choice is made at compile time. */
+enum SumMode { SUM_NONE = 0, SUM_FRIEDMANN = 1, SUM_FULL = 2, SUM_FRIEDMANN_EG = 3 };
+
 /* sums: 0 none, 1 only what the Friedmann update needs, 2 every box average */
 cudaError_t launch_step(int prec, const StepConst &k, bool drift_first, int sums, const void *phi_in,
                         const void *pi_in, void *phi_out, void *pi_out, void *loc_ek, void *loc_eg, void *loc_ep,

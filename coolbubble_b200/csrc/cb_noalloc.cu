@@ -19,7 +19,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "cb_handle.h"
@@ -38,25 +37,16 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 
 namespace {
 
-constexpr int MAX_DEVICES = 64;
-std::mutex g_mu;
-void *g_scratch_addr[MAX_DEVICES] = {};
-
-/* Device address of the scratch array on the current device, looked up once
- * per device (host code cannot pass the symbol itself to a kernel). */
+/* Device address of the scratch array on the current device (host code cannot
+ * pass the symbol itself to a kernel). Looked up on every call, with the
+ * caller's device current: the lookup is cheap next to the synchronisation the
+ * call ends with, and an address cached across calls would go stale if the
+ * application reset the device (cudaDeviceReset reloads the module). */
 int scratch_address(void **out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cb_step_static_noalloc: querying the current device");
-    if (dev < 0 || dev >= MAX_DEVICES) return fail(nullptr, CB_EUNSUPPORTED, "cb_step_static_noalloc: device ordinal too large");
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(nullptr, e, "cb_step_static_noalloc: cudaGetSymbolAddress of the scratch array");
-        g_scratch_addr[dev] = p;
-    }
-    *out = g_scratch_addr[dev];
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cb_step_static_noalloc: cudaGetSymbolAddress of the scratch array");
+    *out = p;
     return CB_OK;
 }
 
@@ -73,6 +63,8 @@ using namespace cb;
 
 extern "C" int cb_step_static_noalloc(const cb_params *p, const void *phi_in, const void *pi_in, void *phi_out,
                                       void *pi_out, double t_in, cb_sums *out) {
+    /* nothing throws across the C ABI (the messages below are std::strings) */
+    return guard(nullptr, [&]() -> int {
     std::string why;
     int r = validate_params(p, why);
     if (r != CB_OK) return fail(nullptr, r, "cb_step_static_noalloc: " + why);
@@ -108,7 +100,7 @@ extern "C" int cb_step_static_noalloc(const cb_params *p, const void *phi_in, co
     cudaError_t e = cudaMemcpyAsync(st, &s, sizeof s, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) {
         const int prec = p->precision == CB_FP64 ? P_FP64 : P_FP32;
-        e = launch_step(prec, k, false, 2, phi_in, pi_in, phi_out, pi_out, nullptr, nullptr, nullptr, st, partials,
+        e = launch_step(prec, k, false, SUM_FULL, phi_in, pi_in, phi_out, pi_out, nullptr, nullptr, nullptr, st, partials,
                         stream);
     }
     DevState res;
@@ -120,4 +112,5 @@ extern "C" int cb_step_static_noalloc(const cb_params *p, const void *phi_in, co
     tmp.t = t_in + p->dt;
     fill_sums(&tmp, res, out);
     return CB_OK;
+    });
 }

@@ -206,12 +206,6 @@ __device__ void set_coefficients(const StepConst &k, DevState *st) {
     st->adx_pow2 = is_pow2(st->adx);
 }
 
-/* Which sums a step kernel accumulates. */
-enum SumMode { SUM_NONE = 0, SUM_FRIEDMANN = 1, SUM_FULL = 2, SUM_FRIEDMANN_EG = 3 };
-/* SUM_FRIEDMANN_EG: the Friedmann sums with the gradient energy (conformal
- * time, alpha = 1); the staged d = 3 kernel takes it as its own variant so
- * the choice is made at compile time. */
-
 /* The six powers of one epilogue, one per lane of the calling warp (they are
  * independent; lanes 6..31 compute a harmless pow(1, 0)). */
 __device__ __forceinline__ double lane_pow(int lane, const double (&base)[6], const double (&ex)[6]) {

@@ -254,9 +254,11 @@ int cb_initial_condition(const cb_params *p, const cb_ic_params *ic, const char 
  * last block finishes the step with -- is a fixed 1 MiB array in the library,
  * reserved on every device that loads it until the process exits; a lattice
  * whose step needs more than its 10912 partial-sum rows is rejected with
- * CB_EINVAL. The first call on a device looks the array's device address up
- * once (cudaGetSymbolAddress); make that first call before any stream
- * capture. All calls share the one array and it keeps the last call's
+ * CB_EINVAL. Every call looks the array's device address up on the current
+ * device (cudaGetSymbolAddress; the first call on a device may also load the
+ * library's kernels there), so the address stays valid across a
+ * cudaDeviceReset of the application's; make the first call on a device
+ * before any stream capture. All calls share the one array and it keeps the last call's
  * contents, so calls that overlap on the GPU (other host threads, other
  * streams) race; each call runs on the default stream and waits for its step. */
 int cb_step_static_noalloc(const cb_params *p, const void *phi_in, const void *pi_in, void *phi_out, void *pi_out,

@@ -24,7 +24,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_bin", "libcboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libcbref.so")
 REF_EXE = os.path.join(HERE, "_ref", "coolbubble_ref")
-REF_SRC = os.environ.get("CB_REFERENCE_SRC", "/root/reference")
+# where the reference sources lie: CB_REFERENCE_SRC, else the checkout beside this repository
+REF_SRC = os.environ.get("CB_REFERENCE_SRC") or os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
 
 SCALAR_NAMES = (
     "t", "a", "ap", "H", "C", "Etot", "Ekintot", "Egradtot", "Epottot", "avphi", "avphiP",

@@ -237,7 +237,7 @@ def test_reference_reader_opens_the_snapshots(tmp_path, monkeypatch):
     the stored thinning stride, t and a."""
     import importlib.util
     import sys
-    ref = os.environ.get("CB_REFERENCE_SRC", "/root/reference")   # where the reference sources lie
+    from oracle.bridge import REF_SRC as ref   # where the reference sources lie
     src = os.path.join(ref, "python", "runfiles.py")
     if not os.path.exists(src):
         pytest.skip("the reference sources are not present")

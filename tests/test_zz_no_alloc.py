@@ -24,6 +24,8 @@ def _dev(a, torch, dtype):
     dict(d=3, n=64, L=16.0, c=4.0, precision="fp64"),     # tiled d = 3 kernel
     dict(d=2, n=96, L=30.0, c=5.0, precision="fp64"),     # generic kernel, exact-division path
     dict(d=3, n=128, L=32.0, c=2.0, precision="fp32c"),
+    dict(d=2, n=1024, L=128.0, c=4.0, precision="fp32c"),   # d = 2 column-strip kernel (from 1024^2 sites)
+    dict(d=1, n=1 << 20, L=131072.0, c=4.0, precision="fp64"),   # the strip kernel on one row (d = 1, 2^20 sites)
 ])
 def test_noalloc_two_steps_match_handle_path(case):
     torch = pytest.importorskip("torch")
