@@ -32,11 +32,11 @@ class cb_ic_params(C.Structure):
 
 class cb_scalars(C.Structure):
     _fields_ = [("t", C.c_double), ("a", C.c_double), ("ap", C.c_double), ("H", C.c_double),
-                ("ekin_half_prev", C.c_double)]
+                ("ekin_half_prev", C.c_double), ("etot0", C.c_double)]
 
 
 SUM_FIELDS = ("t", "a", "H", "C", "etot", "ekin", "egrad", "epot", "etot_var", "ekin_var", "egrad_var", "epot_var",
-              "avphi", "avphi_var", "avphip", "avphip_var", "ap", "ekin_half_prev")
+              "avphi", "avphi_var", "avphip", "avphip_var", "ap", "ekin_half_prev", "w", "etot_drift", "c_rel")
 
 
 class cb_sums(C.Structure):

@@ -49,7 +49,7 @@ class Bubble:
             phi, pi, sc = state
             phi = np.ascontiguousarray(phi, dtype=np.float64).reshape(-1)
             pi = np.ascontiguousarray(pi, dtype=np.float64).reshape(-1)
-            s0 = L.cb_scalars(sc["t"], sc["a"], sc["ap"], sc["H"], sc["ekin_half_prev"])
+            s0 = L.cb_scalars(sc["t"], sc["a"], sc["ap"], sc["H"], sc["ekin_half_prev"], sc.get("etot0", 0.0))
             check(L.lib.cb_create(L.C.byref(params), L.dptr(phi), L.dptr(pi), L.C.byref(s0), L.C.byref(h)))
             s = L.cb_sums()
             s.t, s.a, s.ap, s.H, s.ekin_half_prev = sc["t"], sc["a"], sc["ap"], sc["H"], sc["ekin_half_prev"]

@@ -192,6 +192,9 @@ void fill_sums(const cb_handle *h, const DevState &s, cb_sums *o) {
     o->avphip_var = s.avphip_var;
     o->ap = s.ap;
     o->ekin_half_prev = s.ekin_half_prev;
+    o->w = s.w;
+    o->etot_drift = s.etot_drift;
+    o->c_rel = s.c_rel;
 }
 
 /* Queue a copy of the run's step record into host memory (pinned, so the copy
@@ -597,6 +600,7 @@ int cb_create(const cb_params *p, const double *phi, const double *pi_mhalf, con
     s.H = s0->H;
     s.C = 0.0;
     s.ekin_half_prev = s0->ekin_half_prev;
+    s.etot0 = std::isfinite(s0->etot0) ? s0->etot0 : 0.0;
     s.drift_p = 0.0;
     host_coefficients(h->k, s);
     h->t = s0->t;

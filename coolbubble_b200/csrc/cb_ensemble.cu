@@ -307,28 +307,6 @@ __global__ void k_ensemble2d(const EnsMember *__restrict__ members, int cs, int 
     cluster.sync();
 }
 
-/* Copies the box sums of a handle's last measured step into a record (members stepped on their own). */
-__global__ void k_state_to_record(const DevState *st, double dxLD, EnsRecord *rec) {
-    /* the record holds raw sums: divide the scaled values back (exact for power-of-two dxLD) is not
-       needed -- members stepped on their own store their finished line in rec->v as scaled values,
-       flagged by a negative NSUM-th slot */
-    if (threadIdx.x == 0) {
-        rec->v[S_EK] = st->ekin;
-        rec->v[S_EP] = st->epot;
-        rec->v[S_EG] = st->egrad;
-        rec->v[S_PHI] = st->avphi;
-        rec->v[S_V] = st->avphip;
-        rec->v[Q_EK] = st->ekin_var;
-        rec->v[Q_EP] = st->epot_var;
-        rec->v[Q_EG] = st->egrad_var;
-        rec->v[Q_ET] = st->etot_var;
-        rec->v[Q_PHI] = st->avphi_var;
-        rec->v[Q_V] = st->avphip_var;
-        rec->v[S_EKIN_IN] = -1.0;   /* marks a finished line (already scaled) */
-        (void)dxLD;
-    }
-}
-
 size_t resident_smem(int prec, int n, int cs) {
     const size_t esz = prec == P_FP64 ? 8 : 4;
     return 3 * (size_t)(n / cs) * n * esz;
@@ -382,6 +360,10 @@ std::map<long long, int> g_tuned;
 }  // namespace cb
 
 using namespace cb;
+
+namespace cb {
+void fill_sums(const cb_handle *h, const DevState &s, cb_sums *o);
+}
 
 struct cb_ensemble {
     std::vector<cb_handle *> members;
@@ -574,12 +556,21 @@ int cb_ensemble_step(cb_ensemble *e, int nsteps, int sums_every, cb_sums *out) {
         if (nev > 0 && !out) return fail(nullptr, CB_EINVAL, "cb_ensemble_step: out is NULL");
         const int count = (int)e->members.size();
         EnsRecord *drec = nullptr;
+        DevState *dstate = nullptr;   /* members stepped on their own: their step records at each line */
         if (nev > 0 && cudaMalloc(&drec, (size_t)count * nev * sizeof(EnsRecord)) != cudaSuccess) {
             cudaGetLastError();
             return fail(nullptr, CB_ENOMEM, "cb_ensemble_step: device allocation of the records failed");
         }
+        if (nev > 0 && !e->own.empty() &&
+            cudaMalloc(&dstate, (size_t)count * nev * sizeof(DevState)) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(drec);
+            return fail(nullptr, CB_ENOMEM, "cb_ensemble_step: device allocation of the records failed");
+        }
         std::vector<double> t_start(count);
         for (int i = 0; i < count; ++i) t_start[i] = e->members[i]->t;
+        /* the t = 0 total energy of each member, for the energy drift of its lines */
+        std::vector<double> etot0(count, 0.0);
         cudaError_t err = cudaSuccess;
         /* resident classes: one launch each, on their own streams */
         for (auto &c : e->classes) {
@@ -588,6 +579,11 @@ int cb_ensemble_step(cb_ensemble *e, int nsteps, int sums_every, cb_sums *out) {
                 cb_handle *h = e->members[c.idx[q]];
                 flush_pending(h);
                 cudaStreamSynchronize(h->stream);
+                if (nev > 0 && cudaMemcpy(&etot0[c.idx[q]], &h->st->etot0, sizeof(double), cudaMemcpyDeviceToHost) !=
+                                   cudaSuccess) {
+                    cudaGetLastError();
+                    etot0[c.idx[q]] = 0.0;
+                }
                 host[q].phi = h->phi[h->cphi];
                 host[q].pi = h->pi[h->cpi];
                 host[q].k = h->k;
@@ -612,7 +608,11 @@ int cb_ensemble_step(cb_ensemble *e, int nsteps, int sums_every, cb_sums *out) {
                 int r = step_impl(h, kk, rec ? CB_STEP_SUMS : 0, false);
                 if (r != CB_OK) { err = cudaErrorLaunchFailure; break; }
                 if (rec) {
-                    k_state_to_record<<<1, 32, 0, h->stream>>>(h->st, h->k.dxLD, drec + (size_t)i * nev + j);
+                    if (cudaMemcpyAsync(dstate + (size_t)i * nev + j, h->st, sizeof(DevState),
+                                        cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess) {
+                        err = cudaErrorLaunchFailure;
+                        break;
+                    }
                     ++j;
                 }
                 done += kk;
@@ -621,9 +621,13 @@ int cb_ensemble_step(cb_ensemble *e, int nsteps, int sums_every, cb_sums *out) {
         for (auto &c : e->classes) if (err == cudaSuccess) err = cudaStreamSynchronize(c.stream);
         for (int i : e->own) if (err == cudaSuccess) err = cudaStreamSynchronize(e->members[i]->stream);
         std::vector<EnsRecord> rec((size_t)count * nev);
+        std::vector<DevState> srec(dstate ? (size_t)count * nev : 0);
         if (err == cudaSuccess && nev > 0)
             err = cudaMemcpy(rec.data(), drec, rec.size() * sizeof(EnsRecord), cudaMemcpyDeviceToHost);
+        if (err == cudaSuccess && dstate)
+            err = cudaMemcpy(srec.data(), dstate, srec.size() * sizeof(DevState), cudaMemcpyDeviceToHost);
         cudaFree(drec);
+        if (dstate) cudaFree(dstate);
         if (err != cudaSuccess) return cuda_fail(nullptr, err, "cb_ensemble_step");
         /* lines of the resident members (static background: a = 1, H = C = 0) and times */
         for (int i = 0; i < count; ++i) {
@@ -636,16 +640,13 @@ int cb_ensemble_step(cb_ensemble *e, int nsteps, int sums_every, cb_sums *out) {
                 cb_sums &o = out[(size_t)i * nev + j];
                 const EnsRecord &r = rec[(size_t)i * nev + j];
                 std::memset(&o, 0, sizeof o);
-                o.t = t;
-                o.a = 1.0;
-                if (own || r.v[S_EKIN_IN] < 0) {
-                    o.ekin = r.v[S_EK]; o.epot = r.v[S_EP]; o.egrad = r.v[S_EG];
-                    o.etot = o.ekin + o.epot + o.egrad;
-                    o.avphi = r.v[S_PHI]; o.avphip = r.v[S_V];
-                    o.ekin_var = r.v[Q_EK]; o.epot_var = r.v[Q_EP]; o.egrad_var = r.v[Q_EG]; o.etot_var = r.v[Q_ET];
-                    o.avphi_var = r.v[Q_PHI]; o.avphip_var = r.v[Q_V];
+                if (own) {   /* the member's own step record: the line cb_step gives */
+                    fill_sums(h, srec[(size_t)i * nev + j], &o);
+                    o.t = t;
                     continue;
                 }
+                o.t = t;
+                o.a = 1.0;
                 /* the scalar part of measureEnergies for a = 1 (bubble.cpp:812-843) */
                 const double dxLD = h->k.dxLD, dxLD2 = dxLD * dxLD;
                 const double ekhalf = r.v[S_EK] * dxLD, ekprev = r.v[S_EKIN_IN] * dxLD;
@@ -662,6 +663,17 @@ int cb_ensemble_step(cb_ensemble *e, int nsteps, int sums_every, cb_sums *out) {
                 o.avphi_var = r.v[Q_PHI] * dxLD2;
                 o.avphip_var = r.v[Q_V] * dxLD2;
                 o.ekin_half_prev = ekhalf;
+                /* the line's checks (static background: H = C = 0); a run created without
+                 * its t = 0 energy measures the drift from its first line */
+                if (etot0[i] == 0.0) {
+                    etot0[i] = o.etot;
+                    if (cudaMemcpy(&h->st->etot0, &etot0[i], sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+                        cudaGetLastError();
+                }
+                const LineChecks lc = line_checks(h->p.d, o.ekin, o.egrad, o.epot, o.etot, etot0[i], 0.0, 0.0);
+                o.w = lc.w;
+                o.etot_drift = lc.drift;
+                o.c_rel = 0.0;
             }
             if (!own) {
                 for (; stepped < nsteps; ++stepped) t += h->p.dt;

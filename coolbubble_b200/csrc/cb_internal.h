@@ -48,6 +48,9 @@ struct DevState {
     double etot, ekin, egrad, epot;
     double etot_var, ekin_var, egrad_var, epot_var;
     double avphi, avphi_var, avphip, avphip_var;
+    /* checks of the last measured line: equation of state, energy drift against
+     * etot0 (the t = 0 total energy; 0 until known), C / H^2 */
+    double w, etot_drift, c_rel, etot0;
     /* last-block-done ticket and error word */
     unsigned int counter;
     int err;
@@ -77,6 +80,24 @@ struct StepConst {
     int force_generic;  /* 1: always use the generic tile kernel (diagnostics and cross-checks) */
     int temporal;       /* steps per pass for static float 3-D lattices (1: no temporal blocking) */
 };
+
+/* The checks of one line from its energies, in double and in this order (the
+ * step epilogue does the same operations with explicit rounding):
+ * w = (Ekin - (d-2)/d Egrad - Epot) / Etot (python/plot_SummaryPlots.py:91-95);
+ * drift = Etot / Etot0 - 1 (plot_SummaryPlots.py:80-81), 0 while Etot0 is
+ * unknown; C / H^2 when H != 0. Host code (lines assembled on the host). */
+struct LineChecks {
+    double w, drift, c_rel;
+};
+inline LineChecks line_checks(int d, double ekin, double egrad, double epot, double etot, double etot0, double H,
+                              double C) {
+    LineChecks r;
+    const double q = (double)(d - 2) / (double)d;
+    r.w = (ekin - q * egrad - epot) / etot;
+    r.drift = etot0 != 0.0 ? etot / etot0 - 1.0 : 0.0;
+    r.c_rel = H != 0.0 ? C / (H * H) : 0.0;
+    return r;
+}
 
 /* Kernel launchers (cb_step.cu). Each returns the cudaError_t of the launch. */
 enum Prec { P_FP64 = 0, P_FP32 = 1 };

@@ -307,6 +307,12 @@ __global__ void __launch_bounds__(NT) k_ic_energies(StepConst k, size_t N, const
         st->H = H0;
         st->C = 0.0;
         st->drift_p = 0.0;
+        /* the t = 0 line's checks (the epilogue's formulas): the drift is measured from here */
+        const double q = __ddiv_rn((double)(k.d - 2), (double)k.d);
+        st->w = __ddiv_rn(__dsub_rn(__dsub_rn(st->ekin, __dmul_rn(q, st->egrad)), st->epot), st->etot);
+        st->etot0 = st->etot;
+        st->etot_drift = 0.0;
+        st->c_rel = 0.0;
         set_coefficients(k, st);
     }
 }

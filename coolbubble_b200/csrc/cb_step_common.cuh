@@ -283,8 +283,18 @@ __device__ void epilogue(const StepConst &k, DevState *st, const double *tot, bo
         st->avphip_var = __dmul_rn(tot[Q_V], dxLD2);
     }
     st->H = H;
-    if (full)   /* C needs the full Etot; only reported at steps that measure all sums */
-        st->C = k.expanding ? __dsub_rn(__dmul_rn(H, H), __ddiv_rn(__dmul_rn(pw[0], etot), mpl2)) : 0.0;
+    if (full) { /* C needs the full Etot; only reported at steps that measure all sums */
+        const double C = k.expanding ? __dsub_rn(__dmul_rn(H, H), __ddiv_rn(__dmul_rn(pw[0], etot), mpl2)) : 0.0;
+        st->C = C;
+        /* the line's checks (line_checks in cb_internal.h): equation of state,
+         * energy drift against the t = 0 total (the first measured line sets it
+         * when unknown), Friedmann constraint relative to H^2 */
+        const double q = __ddiv_rn((double)(d - 2), (double)d);
+        st->w = __ddiv_rn(__dsub_rn(__dsub_rn(ekin, __dmul_rn(q, egrad)), epot), etot);
+        if (st->etot0 == 0.0) st->etot0 = etot;
+        st->etot_drift = __dsub_rn(__ddiv_rn(etot, st->etot0), 1.0);
+        st->c_rel = H != 0.0 ? __ddiv_rn(C, __dmul_rn(H, H)) : 0.0;
+    }
     st->a = a;
     st->ap = ap;
     st->drift_p = pw[1];

@@ -66,24 +66,37 @@ typedef struct cb_params {
 } cb_params;
 
 /* State handed to the time loop by the reference constructor
- * (bubble.cpp:271-291): a_0, a'_{-1/2}, H_0 and the kinetic energy at t = -1/2. */
+ * (bubble.cpp:271-291): a_0, a'_{-1/2}, H_0 and the kinetic energy at t = -1/2,
+ * and the total energy at t = 0 (bubble.cpp:263), against which the energy
+ * drift of later lines is measured (0: from the first line a step measures). */
 typedef struct cb_scalars {
     double t;
     double a;
     double ap;
     double H;
     double ekin_half_prev;
+    double etot0;
 } cb_scalars;
 
 /* One line of EnergyDensities.dat (bubble.cpp:977-989) plus the leapfrog
  * scalars. The *_var entries are the raw sums of squares (the reference's
- * static *Var variables, bubble.cpp:44); the file prints their square roots. */
+ * static *Var variables, bubble.cpp:44); the file prints their square roots.
+ * The last three are the run's accuracy and state checks, formed in double on
+ * the device from the same line (the reference's plotting scripts derive them
+ * from the file afterwards):
+ *   w          = (Ekin - (d-2)/d Egrad - Epot) / Etot, the equation of state
+ *                (python/plot_SummaryPlots.py:91-95);
+ *   etot_drift = Etot / Etot(t = 0) - 1, energy conservation in a static
+ *                background (plot_SummaryPlots.py:80-81; README "Accuracy");
+ *   c_rel      = C / H^2, the first Friedmann equation as a constraint in an
+ *                expanding background (bubble.cpp:874-875; 0 when static). */
 typedef struct cb_sums {
     double t, a, H, C;
     double etot, ekin, egrad, epot;
     double etot_var, ekin_var, egrad_var, epot_var;
     double avphi, avphi_var, avphip, avphip_var;
     double ap, ekin_half_prev;
+    double w, etot_drift, c_rel;
 } cb_sums;
 
 typedef struct cb_handle cb_handle;

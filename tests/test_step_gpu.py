@@ -39,6 +39,35 @@ def check_sums(got, ref, N, tol=SUM_TOL, where=""):
     assert abs(got["C"] - ref["C"]) <= tol * max(ref["H"] ** 2, 1e-300), (where, "C", got["C"], ref["C"])
 
 
+def check_scale(key, s):
+    """Scale on which a line's checks compare: the drift Etot/Etot0 - 1 on that
+    of Etot/Etot0 (its error is Etot's relative error), C/H^2 on 1 + |C/H^2|,
+    w on the sum of its terms' magnitudes over |Etot|."""
+    if key == "etot_drift":
+        return 1.0 + abs(s["etot_drift"])
+    if key == "c_rel":
+        return 1.0 + abs(s["c_rel"])
+    if key == "w":
+        return (abs(s["ekin"]) + abs(s["egrad"]) + abs(s["epot"])) / max(abs(s["etot"]), 1e-300)
+    return 0.0
+
+
+def w_of(ref, d):
+    """Equation of state of a reference line (python/plot_SummaryPlots.py:91-95)."""
+    return (ref["Ekintot"] - (d - 2) / d * ref["Egradtot"] - ref["Epottot"]) / ref["Etot"]
+
+
+def check_line_checks(got, ref, d, etot0, tol=SUM_TOL, where=""):
+    """w, the energy drift and C/H^2 of a line against those formed from the
+    reference's own scalars (etot0: the reference's t = 0 total energy)."""
+    w = w_of(ref, d)
+    assert abs(got["w"] - w) <= tol * check_scale("w", got), (where, "w", got["w"], w)
+    drift = ref["Etot"] / etot0 - 1.0
+    assert abs(got["etot_drift"] - drift) <= tol * (1.0 + abs(drift)), (where, "drift", got["etot_drift"], drift)
+    c_rel = ref["C"] / ref["H"] ** 2 if ref["H"] != 0 else 0.0
+    assert abs(got["c_rel"] - c_rel) <= tol * (1.0 + abs(c_rel)), (where, "c_rel", got["c_rel"], c_rel)
+
+
 def params_from(meta, precision="fp64", memorysave=0):
     import coolbubble_b200 as cb
     return cb.make_params(meta["d"], meta["n"], meta["L"], meta["c"], meta["dt"], alpha=meta.get("alpha", 0),
@@ -64,10 +93,13 @@ def test_fp64_matches_reference_golden(name):
                   ("ap", "ap"), ("H", "H"), ("ekin_half_prev", "EkinHalfPrev")):
         assert s.last[k] == pytest.approx(ref0[rk], rel=SUM_TOL, abs=1e-300), k
     N = m["n"] ** m["d"]
+    assert s.last["etot_drift"] == 0.0 and s.last["c_rel"] == 0.0
+    assert abs(s.last["w"] - w_of(ref0, m["d"])) <= SUM_TOL * check_scale("w", s.last)
     for it in range(1, m["steps"] + 1):
         got = s.step(1, sums=True, local=(it == m["steps"]))
         ref = dict(zip(SCALAR_NAMES, g["scalars"][it]))
         check_sums(got, ref, N, where=(name, it))
+        check_line_checks(got, ref, m["d"], ref0["Etot"], where=(name, it))
         assert got["t"] == ref["t"]
     f = s.fields()
     for k in ("phi", "pi", "ekin", "egrad", "epot"):
@@ -83,10 +115,12 @@ def test_dropin_create_from_reference_state(name):
     m = g["meta"]
     sc0 = dict(zip(SCALAR_NAMES, g["scalars"][0]))
     state = (g["phi_start"], g["pi_start"], dict(t=0.0, a=sc0["a"], ap=sc0["ap"], H=sc0["H"],
-                                                  ekin_half_prev=sc0["EkinHalfPrev"]))
+                                                  ekin_half_prev=sc0["EkinHalfPrev"], etot0=sc0["Etot"]))
     s = cb.Bubble(params_from(m), state=state)
     got = s.step(m["steps"], sums=True, local=True)
-    check_sums(got, dict(zip(SCALAR_NAMES, g["scalars"][-1])), m["n"] ** m["d"], where=name)
+    ref = dict(zip(SCALAR_NAMES, g["scalars"][-1]))
+    check_sums(got, ref, m["n"] ** m["d"], where=name)
+    check_line_checks(got, ref, m["d"], sc0["Etot"], where=name)
     f = s.fields()
     for k in ("phi", "pi", "ekin", "egrad", "epot"):
         assert field_err(f[k], g[k + "_end"]) <= FIELD_TOL, k
@@ -228,6 +262,7 @@ def test_tiled_kernel_equals_generic_kernel_fp64(case, monkeypatch):
         scale = abs(b["H"]) ** 2 if key == "C" else abs(b[key])
         if key in ("avphi", "avphip"):
             scale = max(scale, (n ** d * b[key + "_var"]) ** 0.5)
+        scale = max(scale, check_scale(key, b))
         assert abs(a[key] - b[key]) <= 1e-14 * scale + 1e-300, key
     fa, fb = tiled.fields(), generic.fields()
     for key in fa:
@@ -267,6 +302,7 @@ def test_strip_kernel_equals_generic_kernel_2d(d, n, prec, L, monkeypatch):
             scale = abs(b["H"]) ** 2 + abs(b["etot"]) / (3 * 200.0 ** 2) if key == "C" else abs(b[key])
             if key in ("avphi", "avphip"):
                 scale = max(scale, (n ** d * b[key + "_var"]) ** 0.5)
+            scale = max(scale, check_scale(key, b))
             assert abs(a[key] - b[key]) <= tol * scale + 1e-300, key
         fa, fb = strip.fields(), generic.fields()
         for key in fa:
