@@ -12,8 +12,8 @@ the report gives, FP32C against FP64:
   w                           absolute error of (Ekin - (d-2)/d Egrad - Epot) / Etot
   drift                       absolute error of Etot / Etot(0) - 1
   a                           relative error of the scale factor
-  spec_1e8 / 1e7 / 1e6        largest relative error of Delta_phi(k) over the
-                              shells above 1e-8 / 1e-7 / 1e-6 of the peak
+  spec_1e8 .. spec_1e4        largest relative error of Delta_phi(k) over the
+                              shells above 1e-8 .. 1e-4 of the peak
   spec_over_1e4               shells above 1e-8 of the peak whose error exceeds 1e-4
 
 and, for a run with one centred bubble (mode -2, static), the tracked wall:
@@ -91,7 +91,8 @@ def _spec_errors(s64, s32):
     ref, got = pw[m] / ws[m], pw32[m] / ws[m]
     rel = np.abs(got / np.where(ref != 0, ref, 1.0) - 1.0)
     out = {}
-    for name, floor in (("spec_1e8", 1e-8), ("spec_1e7", 1e-7), ("spec_1e6", 1e-6)):
+    for name, floor in (("spec_1e8", 1e-8), ("spec_1e7", 1e-7), ("spec_1e6", 1e-6), ("spec_1e5", 1e-5),
+                        ("spec_1e4", 1e-4)):
         big = ref > floor * ref.max()
         out[name] = float(rel[big].max(initial=0.0))
     big = ref > 1e-8 * ref.max()
