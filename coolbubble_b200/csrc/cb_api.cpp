@@ -356,7 +356,7 @@ int ensure_tmp(cb_handle *h, size_t bytes) {
  * choice is cached per device and lattice size. Both passes give the same
  * fields bit for bit, so the choice only changes the speed. */
 int choose_temporal(cb_handle *h) {
-    if (h->expanding || h->prec != P_FP32 || h->p.d != 3) return 1;
+    if (h->expanding || !h->unit_scale || h->prec != P_FP32 || h->p.d != 3) return 1;
     int tj, ns, parts;
     size_t sm;
     unsigned g;
@@ -474,7 +474,8 @@ int step_impl(cb_handle *h, int nsteps, int flags, bool timed) {
     unsigned g;
     if (h->k.temporal == 0 && nsteps > 2) h->k.temporal = choose_temporal(h);
     const int tl = h->k.temporal;
-    const bool tb_ok = !h->expanding && tl > 1 && step3tb_geometry(h->k, h->prec, tl, tj, ns, sm, g, parts);
+    const bool tb_ok = !h->expanding && h->unit_scale && tl > 1 &&
+                       step3tb_geometry(h->k, h->prec, tl, tj, ns, sm, g, parts);
     for (int it = 1; it <= nsteps;) {
         const int plain_left = nsteps - it + 1 - (want_last ? 1 : 0);
         if (tb_ok && plain_left >= tl) {
@@ -601,6 +602,8 @@ int cb_create(const cb_params *p, const double *phi, const double *pi_mhalf, con
     s.C = 0.0;
     s.ekin_half_prev = s0->ekin_half_prev;
     s.etot0 = std::isfinite(s0->etot0) ? s0->etot0 : 0.0;
+    /* the two-step pass assumes a^(d-2) = a^d = 1 (a static background that started at a = 1) */
+    h->unit_scale = s0->a == 1.0;
     s.drift_p = 0.0;
     host_coefficients(h->k, s);
     h->t = s0->t;

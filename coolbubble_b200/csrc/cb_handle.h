@@ -53,6 +53,7 @@ struct cb_handle {
     long long steps_done = 0;
     long long launches = 0;   /* kernel launches queued by this run */
     bool pending = false;   /* drift-first: phi is one drift behind the whole step */
+    bool unit_scale = true; /* a = 1 for good (static background from a = 1): the two-step pass applies */
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cb::FftState *fft = nullptr;
     cb::SnapshotWriter *writer = nullptr;

@@ -7,26 +7,29 @@
  *
  *  - Tiles of TJ full rows of axis 1 (axis-2 neighbours wrap in shared
  *    memory); work items (plane part, tile) taken from a device-wide queue,
- *    part-major with tiles fastest, one block per SM.
- *  - Input planes arrive by TMA bulk copies into a ring: phi rows
- *    [j0 - 2, j0 + TJ + 2), pi rows [j0 - 1, j0 + TJ + 1) (periodic rows).
- *  - Level 1 (the first step) covers rows [j0 - 1, j0 + TJ + 1) and keeps
- *    phi (all its rows) and pi (the tile's rows) in a 4-plane ring in shared
- *    memory; level 2 (the second step) covers the tile's rows and writes phi
- *    and pi to HBM.
- *  - Streaming along axis 0: when input plane q has landed, level 1 computes
- *    plane q - 1 and level 2 plane q - 3, from level-1 planes finished in
- *    earlier rounds, so one consumer barrier per input plane separates the
- *    levels and the two levels' work interleaves freely between barriers.
+ *    part-major with tiles fastest (the items in flight share their halo rows
+ *    in L2), one block per SM.
+ *  - Input planes arrive by TMA bulk copies into a 4- to 6-stage ring: phi
+ *    rows [j0 - 2, j0 + TJ + 2), pi rows [j0 - 1, j0 + TJ + 1) (periodic).
+ *  - Each consumer thread owns the same positions in every plane (four of the
+ *    tile, one of the two halo rows for some) and marches them along axis 0:
+ *    its own columns of input phi, of level-1 phi and of level-1 pi stay in
+ *    registers, so shared memory holds only what other threads read -- the
+ *    input planes and two level-1 planes (TJ + 2 rows each). That leaves room
+ *    for 8-row tiles at 512^3 (level-1 rows 1.25x the output rows).
+ *  - Round q (input plane q landed): per position, level 1 (the first step) at
+ *    plane q - 1 and level 2 (the second step, to HBM) at plane q - 2; one
+ *    consumer barrier per round orders the level-1 planes' writes and reuse.
+ *    Axis-2 neighbours come from the adjacent lanes by shuffle.
  *  - An item computing planes [p0, p1) streams input planes p0 - 2 .. p1 + 1
  *    (overlapped tiling: neighbouring items recompute the halo, no block
  *    talks to another). The input ring runs on from one item to the next.
- *  - Per-site arithmetic is the single-step kernel's float path (packed
- *    f32x2, same operations in the same order), so two blocked steps give the
- *    fields of two single steps bit for bit.
+ *  - The per-site results are those of the single-step kernel's float path
+ *    (packed f32x2, the same rounded operations), so two blocked steps give
+ *    the fields of two single steps bit for bit.
  *  - Waits are bounded (clock64 limit, sleeping retries); a timed-out block
  *    records an error word; consumer warps leave together (a vote in the
- *    per-plane barrier).
+ *    per-round barrier).
  */
 #include <cuda_runtime.h>
 
@@ -42,46 +45,42 @@ namespace cb {
 
 namespace {
 
-constexpr int TB_MAXT = 704;             /* at most 21 consumer warps + the producer warp */
-constexpr int TB_HDR = 256;               /* full[8], empty[8], item_full[TB_IQ] mbarriers */
+constexpr int TB_MAXT = 512;             /* threads per block (all of them compute) */
+constexpr int TB_NTS = 2;                 /* tile positions per thread */
+constexpr int TB_HDR = 256;               /* full[nstage] mbarriers (nstage <= 8) */
 constexpr int TB_IQ = 8;
-constexpr int L1_SLOTS = 4;               /* level-1 planes kept */
 
-/* consumer-only barrier (id 1) over nc threads, returning whether any of
- * them passed true */
-__device__ __forceinline__ bool tb_consumer_any(bool x, int nc) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.u32 q, %1, 0;\n\t"
-        "bar.red.or.pred p, 1, %2, q;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(r)
-        : "r"((uint32_t)x), "r"(nc)
-        : "memory");
-    return r != 0;
+/* block-wide barrier (bar.red over all threads), returning whether any
+ * thread passed true */
+__device__ __forceinline__ bool tb_any(bool x) { return __syncthreads_or(x ? 1 : 0) != 0; }
+
+/* shared-memory accesses by 32-bit shared address */
+__device__ __forceinline__ float4 lds4(uint32_t a) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
+/* v = shared float at a where pred != 0 (a predicated load: no branch) */
+__device__ __forceinline__ void lds1_if(float &v, uint32_t a, uint32_t pred) {
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %2, 0;\n\t@p ld.shared.f32 %0, [%1];\n\t}"
+                 : "+f"(v)
+                 : "r"(a), "r"(pred));
+}
+__device__ __forceinline__ void sts4(uint32_t a, const float4 &v) {
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+                 : "memory");
 }
 
-struct TbCursor {
-    int s;
-    uint32_t ph;
-    __device__ __forceinline__ void next(int nstage) {
-        if (++s == nstage) {
-            s = 0;
-            ph ^= 1u;
-        }
-    }
-};
 
 /* Packed constants of the static float update (a = 1). */
 struct Pk {
-    F2 fl, idx2, nfv, dt, c2, nc3, c4;
+    F2 idx2, dt, nc2, c3, nc4;
 };
 
 /* One 16-byte vector (sites kk .. kk+3 of one row) of one leapfrog step on the
  * static background: pi' = pi + dt F(phi), phi' = phi + dt pi' (bubble.cpp:
- * 716-743, 853-856, 867-870 with a = 1), as two packed pairs -- the operations
- * and their order of the single-step kernel's packed path. */
+ * 716-743, 853-856, 867-870 with a = 1), as two packed pairs -- the results of
+ * the single-step kernel's packed path bit for bit. */
 __device__ __forceinline__ void update4(const Pk &K, const float4 c, const float4 um, const float4 up, const float4 im,
                                         const float4 ip, float left, float right, const float4 pv, float4 &phi_n,
                                         float4 &pi_n) {
@@ -93,8 +92,12 @@ __device__ __forceinline__ void update4(const Pk &K, const float4 c, const float
         const F2 t1 = f2_add(f2_sub(upp, two), umm);
         const F2 t2 = f2_add(f2_sub(kpp, two), kmm);
         const F2 lap = f2_add(f2_add(t0, t1), t2);
-        const F2 h = f2_fma(cc, f2_fma(cc, K.c4, K.nc3), K.c2);
-        const F2 force = f2_fma(f2_mul(K.fl, lap), K.idx2, f2_mul(K.nfv, f2_mul(cc, h)));
+        /* -V'(f)/f = -(c2 + f (-c3 + f c4)) with every operand negated: the
+         * exact negation of the one-step kernel's rounded h (round to nearest
+         * is symmetric); with a^(d-2) = a^d = 1 the force fma(1 lap, 1/dx^2,
+         * -1 (f h)) is then fma(lap, 1/dx^2, f (-h)), bit for bit */
+        const F2 nh = f2_fma(cc, f2_fma(cc, K.nc4, K.c3), K.nc2);
+        const F2 force = f2_fma(lap, K.idx2, f2_mul(cc, nh));
         pi2 = f2_fma(K.dt, force, pp);
         phi2 = f2_fma(K.dt, pi2, cc);
     };
@@ -107,6 +110,37 @@ __device__ __forceinline__ void update4(const Pk &K, const float4 c, const float
     pi_n = make_float4(f2_lo(pi01), f2_hi(pi01), f2_lo(pi23), f2_hi(pi23));
 }
 
+/* A tile position of a thread (row r1 of the level-1 rows j0 - 1 .. j0 + tj,
+ * vector kv of the row), updated at both levels in every plane of an item,
+ * with its columns along axis 0 kept in registers:
+ *   x_m, x_c  input phi at planes m - 1, m (level 1 at plane m reads phi at
+ *             m + 1 from the stage that just landed);
+ *   y_m, y_c, y_p  level-1 phi at planes m' - 1, m', m' + 1 (level 2 at m');
+ *   z, zz     level-1 pi at planes m', m' + 1.
+ * A halo position (rows j0 - 1, j0 + tj) is updated at level 1 only and
+ * keeps only x_m, x_c. */
+struct Slot {
+    float4 x_m, x_c, y_m, y_c, y_p, z, zz;
+};
+struct HSlot {
+    float4 x_m, x_c;
+};
+
+/* Two leapfrog steps per pass (see the file comment). Thread c owns the tile
+ * positions c and NT + c (NT = tile positions / 2 = threads) and, for
+ * c < 2 n / 4, halo position c (row j0 - 1, then row j0 + tj). Rows hold a
+ * multiple of 32 vectors, so a warp's 32 positions of a slot are 32
+ * consecutive vectors of one row: the axis-2 neighbours come from the next
+ * lanes by shuffle (the end lanes read them from shared memory), and the
+ * branch on the halo slot is uniform across the warp.
+ * The streamed input planes are counted g = 0, 1, ... over all the block's
+ * items (plane g in stage g mod nstage); round g waits for plane g. An item
+ * computing planes [p0, p1) streams planes p0 - 2 .. p1 + 1: its first two
+ * rounds load the register queues, then round q (input plane q) runs, per
+ * position, level 1 at plane q - 1 and level 2 at plane q - 2. Every round
+ * ends with one barrier of all threads; plane g's stage is free once round
+ * g + 1 has ended, so at the start of round g thread 0 issues the copies of
+ * planes up to g + nstage - 2 (no other wait). */
 __global__ void __launch_bounds__(TB_MAXT, 1)
     k_step3_t2(StepConst k, int tj, int nstage, int parts, const float *__restrict__ phi_in,
                const float *__restrict__ pi_in, float *__restrict__ phi_out, float *__restrict__ pi_out,
@@ -114,7 +148,6 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
     constexpr int W = 4;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ int abort_flag;
-    __shared__ int issued_count;
     __shared__ int item_q[TB_IQ];
 
     const int n = k.n;
@@ -122,10 +155,8 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
     const int R0p = tj + 2;                /* input pi rows: j0 - 1 .. j0 + tj */
     const int R1 = tj + 2;                 /* level-1 phi rows: j0 - 1 .. j0 + tj */
     const int stage_n = (R0 + R0p) * n;    /* floats per input stage */
-    const int slot_n = (R1 + tj) * n;      /* floats per level-1 slot: phi rows, then the tile's pi rows */
+    const int slot_n = R1 * n;             /* floats per level-1 slot */
     uint64_t *full = reinterpret_cast<uint64_t *>(smraw);
-    uint64_t *empty = full + 8;
-    uint64_t *item_full = full + 16;
     float *ring = reinterpret_cast<float *>(smraw + TB_HDR);
     float *l1 = ring + (size_t)nstage * stage_n;
 
@@ -134,11 +165,8 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
     const size_t row_bytes = (size_t)n * sizeof(float);
     const size_t plane = (size_t)n * n;
     const uint32_t tx_bytes = (uint32_t)((size_t)(R0 + R0p) * row_bytes);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    /* consumer warps: all but the last warp of the block (the count is chosen
-     * on the host so that each consumer thread gets the same number of
-     * vectors per input plane) */
-    const int NC = blockDim.x - 32, CW = NC / 32;
+    const int lane = threadIdx.x & 31;
+    const int NT = blockDim.x;
     auto item_of = [&](int it, int &t, int &p0, int &p1) {
         const int c = it / ntiles;
         t = it % ntiles;
@@ -146,189 +174,220 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
         p1 = (int)((long long)(c + 1) * n / parts);
     };
 
+    /* ---- the copies (thread 0): planes are issued in stream order; the
+     *      producer's item j is published in item_q[j % TB_IQ] before its
+     *      first plane is issued ---- */
+    int pr_j = 0, pr_it = -1, pr_pl = 0, pr_p1 = 0, pr_j0 = 0;   /* producer: item, next plane */
+    long long issued = 0;                                        /* planes issued so far */
+    int is_stage = 0;                                            /* its stage: issued mod nstage */
+    bool pr_done = false;
+    auto next_item = [&]() {
+        const int cur = (int)atomicAdd(&st->item_next, 1u);
+        pr_it = cur < items ? cur : -1;
+        item_q[pr_j % TB_IQ] = pr_it;
+        ++pr_j;
+        if (pr_it < 0) {
+            pr_done = true;
+            return;
+        }
+        int t, p0, p1;
+        item_of(pr_it, t, p0, p1);
+        pr_pl = p0 - 2;
+        pr_p1 = p1;
+        pr_j0 = t * tj;
+    };
+    auto issue_upto = [&](long long last) {
+        while (!pr_done && issued <= last) {
+            const int s = is_stage;
+            const int pw = pr_pl < 0 ? pr_pl + n : (pr_pl >= n ? pr_pl - n : pr_pl);
+            float *dst = ring + (size_t)s * stage_n;
+            float *dpi = dst + (size_t)R0 * n;
+            const float *gphi = phi_in + (size_t)pw * plane;
+            const float *gpi = pi_in + (size_t)pw * plane;
+            const int j0 = pr_j0;
+            fence_proxy_async();
+            mbar_arrive_expect_tx(&full[s], tx_bytes);
+            for (int e = 0; e < 2; ++e) {
+                const int ra = (j0 - 2 + e + n) % n, rb = (j0 + tj + e) % n;
+                bulk_g2s(dst + (size_t)e * n, gphi + (size_t)ra * n, (uint32_t)row_bytes, &full[s]);
+                bulk_g2s(dst + (size_t)(2 + tj + e) * n, gphi + (size_t)rb * n, (uint32_t)row_bytes, &full[s]);
+            }
+            bulk_g2s(dst + (size_t)2 * n, gphi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
+            bulk_g2s(dpi, gpi + (size_t)((j0 - 1 + n) % n) * n, (uint32_t)row_bytes, &full[s]);
+            bulk_g2s(dpi + n, gpi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
+            bulk_g2s(dpi + (size_t)(1 + tj) * n, gpi + (size_t)((j0 + tj) % n) * n, (uint32_t)row_bytes, &full[s]);
+            ++issued;
+            if (++is_stage == nstage) is_stage = 0;
+            if (++pr_pl > pr_p1 + 1) next_item();
+        }
+    };
+
     if (threadIdx.x == 0) {
         abort_flag = 0;
-        issued_count = 0;
-        for (int s = 0; s < nstage; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], CW);
-        }
-        for (int s = 0; s < TB_IQ; ++s) mbar_init(&item_full[s], 1);
+        for (int s = 0; s < nstage; ++s) mbar_init(&full[s], 1);
         fence_mbar_init();
     }
     __syncthreads();
     pdl_wait();          /* the previous step's fields, device state and work queue */
+    if (threadIdx.x == 0) {
+        next_item();
+        issue_upto(nstage - 2);
+    }
+    __syncthreads();
 
-    if (warp == CW) {
-        /* ---- producer: each item's input planes p0 - 2 .. p1 + 1 ---- */
-        if (lane == 0) {
-            TbCursor pc{0, 0u};
-            bool wrapped = false;
-            int q = 0;
-            bool ok = true;
-            int cur = (int)atomicAdd(&st->item_next, 1u);
-            for (int j = 0; ok; ++j) {
-                /* the ring keeps the producer within two items of the consumers */
-                item_q[j % TB_IQ] = cur < items ? cur : -1;
-                mbar_arrive(&item_full[j % TB_IQ]);
-                if (cur >= items) break;
-                int t, p0, p1;
-                item_of(cur, t, p0, p1);
-                const int j0 = t * tj;
-                for (int pl = p0 - 2; pl <= p1 + 1; ++pl, ++q) {
-                    if (wrapped && !mbar_wait(&empty[pc.s], pc.ph ^ 1u, WAIT_LIMIT)) {
-                        atomicExch(&abort_flag, 1);
-                        ok = false;
-                        break;
-                    }
-                    if (abort_flag) {
-                        ok = false;
-                        break;
-                    }
-                    const int pw = pl < 0 ? pl + n : (pl >= n ? pl - n : pl);
-                    float *dst = ring + (size_t)pc.s * stage_n;
-                    float *dpi = dst + (size_t)R0 * n;
-                    const float *gphi = phi_in + (size_t)pw * plane;
-                    const float *gpi = pi_in + (size_t)pw * plane;
-                    fence_proxy_async();
-                    mbar_arrive_expect_tx(&full[pc.s], tx_bytes);
-                    for (int e = 0; e < 2; ++e) {
-                        const int ra = (j0 - 2 + e + n) % n, rb = (j0 + tj + e) % n;
-                        bulk_g2s(dst + (size_t)e * n, gphi + (size_t)ra * n, (uint32_t)row_bytes, &full[pc.s]);
-                        bulk_g2s(dst + (size_t)(2 + tj + e) * n, gphi + (size_t)rb * n, (uint32_t)row_bytes,
-                                 &full[pc.s]);
-                    }
-                    bulk_g2s(dst + (size_t)2 * n, gphi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[pc.s]);
-                    bulk_g2s(dpi, gpi + (size_t)((j0 - 1 + n) % n) * n, (uint32_t)row_bytes, &full[pc.s]);
-                    bulk_g2s(dpi + n, gpi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[pc.s]);
-                    bulk_g2s(dpi + (size_t)(1 + tj) * n, gpi + (size_t)((j0 + tj) % n) * n, (uint32_t)row_bytes,
-                             &full[pc.s]);
-                    pc.next(nstage);
-                    if (pc.s == 0) wrapped = true;
-                }
-                /* the next item is taken once this one is fully issued */
-                if (ok) cur = (int)atomicAdd(&st->item_next, 1u);
-            }
-            issued_count = q;
+    Pk K;
+    K.idx2 = f2_splat(k.inv_dx2f);
+    K.dt = f2_splat(k.dtf);
+    K.nc2 = f2_splat(-k.c2f);
+    K.c3 = f2_splat(k.c3f);
+    K.nc4 = f2_splat(-k.c4f);
+    const int nvr = n / W;                     /* vectors per row (a multiple of 32) */
+    /* the positions as offsets r1 n + kk in an array of level-1 rows (row r1,
+     * first site kk; rows hold n = W nvr sites, so tile position u sits at
+     * n + W u): tile slot s at off0 + s W NT, the halo slot at offh */
+    const int off0 = n + W * threadIdx.x, slot_step = W * NT;
+    const bool has_h = threadIdx.x < 2 * nvr;
+    const int offh = W * threadIdx.x + (threadIdx.x < nvr ? 0 : tj * n);
+    const uint32_t first_lane = lane == 0, last_lane = lane == 31;
+    /* every slot of a thread starts at the same site of its row (the slots are
+     * whole rows apart: tj is even), kk = W threadIdx.x mod n; the periodic
+     * wrap of its axis-2 neighbours, for the lanes that read them */
+    const int kk_own = (W * threadIdx.x) % n;
+    const int ladj = kk_own == 0 ? n : 0, radj = kk_own + W == n ? -n : 0;
+    /* the axis-2 neighbours of the vector at shared byte address a: from the
+     * neighbouring lanes, the warp's end lanes from the row */
+    const int ladj_b = 4 * (ladj - 1), radj_b = 4 * (radj + W);
+    auto sides = [&](const float4 &c, uint32_t a, float &left, float &right) {
+        left = __shfl_up_sync(0xffffffffu, c.w, 1);
+        right = __shfl_down_sync(0xffffffffu, c.x, 1);
+        lds1_if(left, a + ladj_b, first_lane);
+        lds1_if(right, a + radj_b, last_lane);
+    };
+    const uint32_t ring_a = smem_u32(ring), l1_a = smem_u32(l1);
+    const uint32_t stage_b = 4u * (uint32_t)stage_n, slot_b = 4u * (uint32_t)slot_n, nb = 4u * (uint32_t)n;
+    const uint32_t pi_b = 4u * (uint32_t)(R0 * n);
+    /* the stage and phase parity of round g's plane, advanced once per round */
+    int gs = 0, gs_prev = 0;
+    uint32_t gph = 0u;
+    auto advance = [&]() {
+        gs_prev = gs;
+        if (++gs == nstage) {
+            gs = 0;
+            gph ^= 1u;
         }
-    } else {
-        /* ---- consumers ---- */
-        Pk K;
-        K.fl = f2_splat((float)st->fl);
-        K.idx2 = f2_splat(k.inv_dx2f);
-        K.nfv = f2_splat(-(float)st->fv);
-        K.dt = f2_splat(k.dtf);
-        K.c2 = f2_splat(k.c2f);
-        K.nc3 = f2_splat(-k.c3f);
-        K.c4 = f2_splat(k.c4f);
-        const int nvr = n / W;                     /* vectors per row */
-        const int V1 = R1 * nvr, V2 = tj * nvr;    /* vectors of level 1 and level 2 per plane */
-        const int nvr_shift = (nvr & (nvr - 1)) == 0 ? __ffs(nvr) - 1 : -1;
-        auto acquire = [&](const TbCursor &c) -> bool {
-            const bool ok = abort_flag == 0 && mbar_wait(&full[c.s], c.ph, WAIT_LIMIT);
-            if (!ok) atomicExch(&abort_flag, 1);
-            return ok;
-        };
-        /* One round: vectors [0, n1) are level 1 (rows j0 - 1 .. j0 + tj of the
-         * planes under the input cursors, into level-1 slot D1), vectors
-         * [n1, n1 + n2) level 2 (the tile's rows from level-1 slots Lm, L0, Lp,
-         * into HBM at g). Row r of a level reads phi rows r, r + 1, r + 2 of its
-         * source planes (centre row r + 1) and pi row r. */
-        auto round = [&](int n1, const float *Sm, const float *S0, const float *Sp, float *D1, int n2,
-                         const float *Lm, const float *L0, const float *Lp, size_t g) {
-            for (int v = threadIdx.x; v < n1 + n2; v += NC) {
-                const bool one = v < n1;
-                const int u = one ? v : v - n1;
-                const int r = nvr_shift >= 0 ? (u >> nvr_shift) : u / nvr;
-                const int kk = (u - r * nvr) * W;
-                const float *A = one ? Sm : Lm, *B = one ? S0 : L0, *C = one ? Sp : Lp;
-                const float *P = B + (one ? R0 : R1) * n;
-                const int c_off = (r + 1) * n + kk;
-                const float4 c = *reinterpret_cast<const float4 *>(B + c_off);
-                const float4 um = *reinterpret_cast<const float4 *>(B + c_off - n);
-                const float4 up = *reinterpret_cast<const float4 *>(B + c_off + n);
-                const float4 im = *reinterpret_cast<const float4 *>(A + c_off);
-                const float4 ip = *reinterpret_cast<const float4 *>(C + c_off);
-                const float4 pv = *reinterpret_cast<const float4 *>(P + r * n + kk);
-                const float left = B[(r + 1) * n + (kk == 0 ? n - 1 : kk - 1)];
-                const float right = B[(r + 1) * n + (kk + W == n ? 0 : kk + W)];
-                float4 phi_n, pi_n;
-                update4(K, c, um, up, im, ip, left, right, pv, phi_n, pi_n);
-                if (one) {
-                    *reinterpret_cast<float4 *>(D1 + r * n + kk) = phi_n;
-                    if (r >= 1 && r <= tj) *reinterpret_cast<float4 *>(D1 + (R1 + r - 1) * n + kk) = pi_n;
-                } else {
-                    *reinterpret_cast<float4 *>(phi_out + g + (size_t)r * n + kk) = phi_n;
-                    *reinterpret_cast<float4 *>(pi_out + g + (size_t)r * n + kk) = pi_n;
+    };
+    /* round g: wait for input plane g; false (and the abort flag) if the wait ran out */
+    auto acquire = [&]() -> bool {
+        const bool ok = abort_flag == 0 && mbar_wait(&full[gs], gph, WAIT_LIMIT);
+        if (!ok) atomicExch(&abort_flag, 1);
+        return ok;
+    };
+    /* end of round g: every thread's reads of the planes and level-1 slots are
+     * done and its level-1 writes visible; thread 0 then issues the planes
+     * whose stages that freed. Returns whether any thread's wait ran out. */
+    auto end_round = [&](long long g, bool bad) -> bool {
+        const bool any_bad = tb_any(bad);
+        if (!any_bad && threadIdx.x == 0) issue_upto(g + nstage - 1);
+        return any_bad;
+    };
+    Slot sl[TB_NTS];
+    HSlot hs;
+    long long g = 0;     /* the round: index of the input plane it waits for */
+    bool bad = false;
+    for (int j = 0;; ++j) {
+        const int it = item_q[j % TB_IQ];
+        if (it < 0) break;
+        int t, p0, p1;
+        item_of(it, t, p0, p1);
+        const int j0 = t * tj;
+        /* input planes p0 - 2 and p0 - 1: this thread's phi into the register queues */
+        if (!bad && acquire()) {
+            const uint32_t S = ring_a + gs * stage_b + nb;
+#pragma unroll
+            for (int s = 0; s < TB_NTS; ++s) sl[s].x_m = lds4(S + 4u * (off0 + s * slot_step));
+            if (has_h) hs.x_m = lds4(S + 4u * offh);
+        } else {
+            bad = true;
+        }
+        if (end_round(g, bad)) break;
+        ++g;
+        advance();
+        if (!bad && acquire()) {
+            const uint32_t S = ring_a + gs * stage_b + nb;
+#pragma unroll
+            for (int s = 0; s < TB_NTS; ++s) sl[s].x_c = lds4(S + 4u * (off0 + s * slot_step));
+            if (has_h) hs.x_c = lds4(S + 4u * offh);
+        } else {
+            bad = true;
+        }
+        if (end_round(g, bad)) break;
+        ++g;
+        advance();
+        for (int q = p0; q <= p1 + 1; ++q, ++g, advance()) {
+            if (!bad && acquire()) {
+                const uint32_t Sn = ring_a + gs * stage_b;        /* plane q */
+                const uint32_t S0 = ring_a + gs_prev * stage_b;   /* plane q - 1 */
+                const uint32_t D1 = l1_a + ((q - p0) & 1) * slot_b;   /* level-1 plane q - 1 */
+                /* level 1 at plane q - 1, at one position with input queue (xm, xc) */
+                auto level1 = [&](float4 &xm, float4 &xc, int off, float4 &phi1, float4 &pi1) {
+                    /* input phi row 0 is level-1 row -1: the centre sits at n + off */
+                    const uint32_t ob = 4u * (uint32_t)off;
+                    const float4 x_p = lds4(Sn + nb + ob);
+                    const float4 um = lds4(S0 + ob);
+                    const float4 up = lds4(S0 + 2u * nb + ob);
+                    const float4 pv = lds4(S0 + pi_b + ob);
+                    float left, right;
+                    sides(xc, S0 + nb + ob, left, right);
+                    update4(K, xc, um, up, xm, x_p, left, right, pv, phi1, pi1);
+                    sts4(D1 + ob, phi1);
+                    xm = xc;
+                    xc = x_p;
+                };
+                /* level 2 at plane q - 2 (from level-1 planes q - 3 .. q - 1) at one tile
+                 * position; level-1 plane q - 2 was written in the last round */
+                const int m2 = q - 2;
+                const uint32_t L0 = l1_a + ((m2 - p0 + 1) & 1) * slot_b;
+                /* global row j0 - 1 + r1 of plane m2: the tile position's offset from row j0 - 1 */
+                const size_t gbase = ((size_t)m2 * n + (size_t)j0) * n - (size_t)n;
+                auto level2 = [&](Slot &x, int off) {
+                    const uint32_t ob = L0 + 4u * (uint32_t)off;
+                    const float4 um = lds4(ob - nb);
+                    const float4 up = lds4(ob + nb);
+                    float left, right;
+                    sides(x.y_c, ob, left, right);
+                    float4 phi2, pi2;
+                    update4(K, x.y_c, um, up, x.y_m, x.y_p, left, right, x.z, phi2, pi2);
+                    *reinterpret_cast<float4 *>(phi_out + (gbase + off)) = phi2;
+                    *reinterpret_cast<float4 *>(pi_out + (gbase + off)) = pi2;
+                };
+                /* per tile position: level 1 at plane q - 1, then level 2 at plane q - 2,
+                 * which needs the position's own level-1 plane q - 1 just computed */
+#pragma unroll
+                for (int s = 0; s < TB_NTS; ++s) {
+                    Slot &x = sl[s];
+                    const int off = off0 + s * slot_step;
+                    float4 phi1, pi1;
+                    level1(x.x_m, x.x_c, off, phi1, pi1);
+                    x.y_m = x.y_c;
+                    x.y_c = x.y_p;
+                    x.y_p = phi1;
+                    x.z = x.zz;
+                    x.zz = pi1;
+                    if (m2 >= p0) level2(x, off);
                 }
+                if (has_h) {
+                    float4 phi1, pi1;
+                    level1(hs.x_m, hs.x_c, offh, phi1, pi1);
+                }
+            } else {
+                bad = true;
             }
-        };
-        bool run = true;
-        TbCursor cq{0, 0u};   /* input cursor of the item's first plane */
-        for (int j = 0; run; ++j) {
-            if (abort_flag != 0 || !mbar_wait(&item_full[j % TB_IQ], (uint32_t)((j / TB_IQ) & 1), WAIT_LIMIT)) {
-                atomicExch(&abort_flag, 1);
-                run = false;
-            }
-            if (tb_consumer_any(!run, NC)) {
-                run = false;
+            if (end_round(g, bad)) {
+                bad = true;
                 break;
             }
-            const int it = item_q[j % TB_IQ];
-            if (it < 0) break;
-            int t, p0, p1;
-            item_of(it, t, p0, p1);
-            const int j0 = t * tj;
-            /* input cursors of planes q - 2, q - 1, q (q: the newest input plane) */
-            TbCursor ca = cq, cb = cq, cc = cq;
-            bool bad = false;
-            for (int q = p0 - 2; q <= p1 + 2; ++q) {
-                if (q <= p1 + 1) {
-                    /* advance the window to input plane q */
-                    if (q == p0 - 2) {
-                        cc = cq;
-                    } else {
-                        ca = cb;
-                        cb = cc;
-                        cc.next(nstage);
-                    }
-                    if (!bad && !acquire(cc)) bad = true;
-                }
-                if (!bad) {
-                    /* level 1 at plane q - 1 from input planes q - 2 .. q; level 2
-                     * at plane p = q - 3 from level-1 planes p - 1 .. p + 1 (level-1
-                     * plane m sits in slot (m - p0 + 1) mod 4) */
-                    const bool do1 = q - 1 >= p0 - 1 && q - 1 <= p1 && q <= p1 + 1;
-                    const int p = q - 3;
-                    const bool do2 = p >= p0 && p < p1;
-                    const int s1 = (q - p0) & (L1_SLOTS - 1);
-                    round(do1 ? V1 : 0, ring + (size_t)ca.s * stage_n, ring + (size_t)cb.s * stage_n,
-                          ring + (size_t)cc.s * stage_n, l1 + (size_t)s1 * slot_n, do2 ? V2 : 0,
-                          l1 + (size_t)((s1 + 1) & (L1_SLOTS - 1)) * slot_n,
-                          l1 + (size_t)((s1 + 2) & (L1_SLOTS - 1)) * slot_n,
-                          l1 + (size_t)((s1 + 3) & (L1_SLOTS - 1)) * slot_n, ((size_t)p * n + j0) * n);
-                }
-                /* input plane q - 2 has had its last use (level 1 at plane q - 1);
-                 * the round after the last input plane only runs level 2 */
-                if (q >= p0 && q <= p1 + 1 && !bad) {
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&empty[ca.s]);
-                }
-                if (tb_consumer_any(bad, NC)) {
-                    run = false;
-                    break;
-                }
-            }
-            if (!run) break;
-            /* the item's last two input planes p1 and p1 + 1 (under cb, cc) */
-            __syncwarp();
-            if (lane == 0) {
-                mbar_arrive(&empty[cb.s]);
-                mbar_arrive(&empty[cc.s]);
-            }
-            cq = cc;
-            cq.next(nstage);
         }
+        if (bad) break;
     }
     __syncthreads();
     /* this block's items are done: the next step may be scheduled */
@@ -341,11 +400,11 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
         }
     }
     if (abort_flag) {
+        /* record, then let every issued copy land before the block exits */
         if (threadIdx.x == 0) {
             atomicExch(&st->err, ERR_TMA_TIMEOUT);
-            const int q1 = issued_count;
-            for (int q = q1 > nstage ? q1 - nstage : 0; q < q1; ++q)
-                mbar_wait(&full[q % nstage], (uint32_t)((q / nstage) & 1), WAIT_LIMIT / 8);
+            for (long long q = issued > nstage ? issued - nstage : 0; q < issued; ++q)
+                mbar_wait(&full[(int)(q % nstage)], (uint32_t)((q / nstage) & 1), WAIT_LIMIT / 8);
         }
         __syncthreads();
     }
@@ -355,36 +414,50 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
 
 int sm_count();
 
+/* Threads of the two-step pass: TB_NTS tile positions each (tj rows of n / 4
+ * vectors); 0 when that is not a whole number of warps or the halo rows'
+ * 2 n / 4 positions outnumber the threads. */
+int step3tb_consumers(int n, int tj) {
+    const int v2 = tj * (n / 4);
+    if (v2 % (32 * TB_NTS) != 0 || v2 / TB_NTS < 2 * (n / 4)) return 0;
+    return v2 / TB_NTS;
+}
+
 /* Geometry of the two-step pass: float fields, d = 3, static background,
- * n a multiple of 4 in [64, 1024]. TJ rows with TJ * n about 2048 sites (4
- * at 512^3, 8 at 256^3); shared memory = the input ring (4..6 stages) + the
- * 4 level-1 planes, one block per SM; the number of plane parts minimises
- * whole rounds of items over the SMs times an item's planes (measured: 9
- * parts at 256^3, 8 at 512^3). */
+ * n a multiple of 128 (rows of a multiple of 32 vectors). TJ rows per tile:
+ * the largest divisor of n (at most 32) whose shared memory -- 4 to 6 input
+ * stages of (2 TJ + 6) rows and 2 level-1 planes of TJ + 2 rows -- fits the
+ * 227 KB of one block per SM, with at most 16 warps (two tile positions
+ * per thread): 8 rows at 512^3, 16 at 256^3. The number of plane
+ * parts minimises whole rounds of items over the SMs times an item's
+ * rounds (its planes plus two). */
 bool step3tb_geometry(const StepConst &k, int prec, int tl, int &tj, int &nstage, size_t &smem, unsigned &grid,
                       int &parts) {
     if (k.d != 3 || prec != P_FP32 || k.expanding || tl != 2) return false;
     const int n = k.n;
-    if (n % 4 != 0 || n < 64 || n > 1024) return false;
+    if (n % 128 != 0 || n > 1024) return false;
     const size_t esz = 4;
-    const size_t budget = 225 * 1024;
-    tj = 1;
-    for (int t = 1; t <= n && t * n <= 2048; ++t)
-        if (n % t == 0) tj = t;
+    const size_t budget = 227 * 1024 - 1024;   /* dynamic share of 227 KB, room for the static variables */
+    tj = 0;
+    for (int t = 2; t <= 32 && t <= n; ++t) {
+        if (n % t != 0) continue;
+        const size_t stage = (size_t)(2 * t + 6) * n * esz;
+        const size_t lev = (size_t)2 * (t + 2) * n * esz;
+        const int nc = step3tb_consumers(n, t);
+        if (TB_HDR + lev + 4 * stage <= budget && nc > 0 && nc <= TB_MAXT) tj = t;
+    }
+    if (tj == 0) return false;
     const size_t stage = (size_t)(2 * tj + 6) * n * esz;
-    const size_t lev = (size_t)L1_SLOTS * (2 * tj + 2) * n * esz;
-    if (budget < TB_HDR + lev + 4 * stage) return false;
+    const size_t lev = (size_t)2 * (tj + 2) * n * esz;
     nstage = (int)((budget - TB_HDR - lev) / stage);
     if (nstage > 6) nstage = 6;
     smem = TB_HDR + (size_t)nstage * stage + lev;
     const long long ntiles = n / tj;
     const long long slots = sm_count();
-    /* whole rounds of items over the SMs (one block each), an item costing
-     * its planes plus about one plane */
     double best = 1e300;
     parts = 1;
     for (int P = 1; P <= n / 4; ++P) {
-        const double per_item = (double)n / P + 1.0;
+        const double per_item = (double)n / P + 2.0;
         const long long rounds = (ntiles * P + slots - 1) / slots;
         const double cost = (double)rounds * per_item;
         if (cost < best - 1e-9) {
@@ -399,27 +472,6 @@ bool step3tb_geometry(const StepConst &k, int prec, int tl, int &tj, int &nstage
     return true;
 }
 
-/* Consumer threads of the two-step pass: a multiple of 32 near (vectors of
- * both levels per input plane) / k, k = 2 (or 1, 3, 4), so that every
- * consumer thread has the same number of vectors in a round; at most 21
- * consumer warps. */
-int step3tb_consumers(const StepConst &k, int tj) {
-    const int nvr = k.n / 4;
-    const int vt = (2 * tj + 2) * nvr;
-    int best = 0;
-    double best_waste = 1e300;
-    for (int per : {2, 3, 1, 4}) {
-        const int nc = ((vt + per - 1) / per + 31) / 32 * 32;
-        if (nc < 256 || nc > TB_MAXT - 32) continue;
-        const double waste = (double)(per * nc - vt) / vt;
-        if (waste < best_waste - 1e-9) {
-            best_waste = waste;
-            best = nc;
-        }
-    }
-    return best ? best : 512;
-}
-
 cudaError_t launch_step3_tb(int prec, const StepConst &k, int tl, const void *phi_in, const void *pi_in,
                             void *phi_out, void *pi_out, DevState *st, cudaStream_t s) {
     int tj, nstage, parts;
@@ -428,8 +480,8 @@ cudaError_t launch_step3_tb(int prec, const StepConst &k, int tl, const void *ph
     if (!step3tb_geometry(k, prec, tl, tj, nstage, smem, grid, parts)) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(k_step3_t2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const int nc = step3tb_consumers(k, tj);
-    return launch_pdl(k_step3_t2, dim3(grid), dim3(nc + 32), smem, s, k, tj, nstage, parts, (const float *)phi_in,
+    const int nc = step3tb_consumers(k.n, tj);
+    return launch_pdl(k_step3_t2, dim3(grid), dim3(nc), smem, s, k, tj, nstage, parts, (const float *)phi_in,
                       (const float *)pi_in, (float *)phi_out, (float *)pi_out, st);
 }
 

@@ -381,18 +381,18 @@ def test_device_error_word_stays_clear():
     assert s.device_error() == 0
 
 
-@pytest.mark.parametrize("n,L,steps", [(64, 16.0, 41), (96, 24.0, 40), (128, 32.0, 40), (256, 32.0, 80),
-                                       (512, 64.0, 9)])
+@pytest.mark.parametrize("n,L,steps", [(128, 32.0, 41), (256, 32.0, 80), (384, 48.0, 21), (512, 64.0, 9)])
 @pytest.mark.parametrize("tl", [2])
 def test_temporal_blocking_matches_single_step_passes(n, L, steps, tl, monkeypatch):
     """Static float 3-D runs: two steps per HBM pass give the fields of one
     step per pass bit for bit (same per-site arithmetic) and energies within
-    the FP32C bar."""
+    the FP32C bar. Sizes: 32-, 16- and 8-row tiles (128^3, 256^3, 512^3), a
+    row of 96 vectors (384^3), odd step counts (a last single step)."""
     import coolbubble_b200 as cb
     from oracle import bridge as B
     d, c = 3, 2.0
     dt = 0.1 * L / n
-    if n > 256:                         # white noise: the band-limited field's 512^3 FFT is slow on the host
+    if n > 256:                         # white noise: the band-limited field's FFT is slow on the host at this size
         rng = np.random.default_rng(31)
         phi0, pi0 = 0.3 * rng.random(n ** d), 0.05 * rng.standard_normal(n ** d)
     else:
@@ -466,3 +466,15 @@ def test_temporal_block_autotuner_keeps_the_fields(monkeypatch):
     fa, fb = auto.fields(local=False), single.fields(local=False)
     for k in ("phi", "pi"):
         np.testing.assert_array_equal(fa[k], fb[k])
+
+
+def test_temporal_blocking_falls_back_where_it_does_not_apply(monkeypatch):
+    """Rows that are not a multiple of 32 vectors (n % 128 != 0) take one-step
+    passes even when two-step passes are asked for."""
+    import coolbubble_b200 as cb
+    d, n, L, c = 3, 96, 24.0, 2.0
+    p = cb.make_params(d, n, L, c, 0.1 * L / n, precision="fp32c", memorysave=1)
+    monkeypatch.setenv("CB_TEMPORAL_BLOCK", "2")
+    s = cb.Bubble(p, smooth_noise(d, n, 0.3, seed=31), smooth_noise(d, n, 0.05, seed=32))
+    s.step(10, sums=True)
+    assert s.counters() == (10, 10)
