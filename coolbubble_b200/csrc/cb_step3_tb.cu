@@ -81,34 +81,101 @@ struct Pk {
  * static background: pi' = pi + dt F(phi), phi' = phi + dt pi' (bubble.cpp:
  * 716-743, 853-856, 867-870 with a = 1), as two packed pairs -- the results of
  * the single-step kernel's packed path bit for bit. */
+/* One packed pair of sites (two neighbours along axis 2): the force with the
+ * periodic Laplacian and V'(phi), the kick and the drift. */
+__device__ __forceinline__ void upd_pair(const Pk &K, F2 cc, F2 umm, F2 upp, F2 imm, F2 ipp, F2 kmm, F2 kpp, F2 pp,
+                                         F2 &phi2, F2 &pi2) {
+    const F2 two = f2_add(cc, cc);
+    const F2 t0 = f2_add(f2_sub(ipp, two), imm);
+    const F2 t1 = f2_add(f2_sub(upp, two), umm);
+    const F2 t2 = f2_add(f2_sub(kpp, two), kmm);
+    const F2 lap = f2_add(f2_add(t0, t1), t2);
+    /* -V'(f)/f = -(c2 + f (-c3 + f c4)) with every operand negated: the
+     * exact negation of the one-step kernel's rounded h (round to nearest
+     * is symmetric); with a^(d-2) = a^d = 1 the force fma(1 lap, 1/dx^2,
+     * -1 (f h)) is then fma(lap, 1/dx^2, f (-h)), bit for bit */
+    const F2 nh = f2_fma(cc, f2_fma(cc, K.nc4, K.c3), K.nc2);
+    const F2 force = f2_fma(lap, K.idx2, f2_mul(cc, nh));
+    pi2 = f2_fma(K.dt, force, pp);
+    phi2 = f2_fma(K.dt, pi2, cc);
+}
+
 __device__ __forceinline__ void update4(const Pk &K, const float4 c, const float4 um, const float4 up, const float4 im,
                                         const float4 ip, float left, float right, const float4 pv, float4 &phi_n,
                                         float4 &pi_n) {
     const F2 c01 = f2_pack(c.x, c.y), c23 = f2_pack(c.z, c.w);
     const F2 km01 = f2_pack(left, c.x), mid = f2_pack(c.y, c.z), kp23 = f2_pack(c.w, right);
-    auto pair = [&](F2 cc, F2 umm, F2 upp, F2 imm, F2 ipp, F2 kmm, F2 kpp, F2 pp, F2 &phi2, F2 &pi2) {
-        const F2 two = f2_add(cc, cc);
-        const F2 t0 = f2_add(f2_sub(ipp, two), imm);
-        const F2 t1 = f2_add(f2_sub(upp, two), umm);
-        const F2 t2 = f2_add(f2_sub(kpp, two), kmm);
-        const F2 lap = f2_add(f2_add(t0, t1), t2);
-        /* -V'(f)/f = -(c2 + f (-c3 + f c4)) with every operand negated: the
-         * exact negation of the one-step kernel's rounded h (round to nearest
-         * is symmetric); with a^(d-2) = a^d = 1 the force fma(1 lap, 1/dx^2,
-         * -1 (f h)) is then fma(lap, 1/dx^2, f (-h)), bit for bit */
-        const F2 nh = f2_fma(cc, f2_fma(cc, K.nc4, K.c3), K.nc2);
-        const F2 force = f2_fma(lap, K.idx2, f2_mul(cc, nh));
-        pi2 = f2_fma(K.dt, force, pp);
-        phi2 = f2_fma(K.dt, pi2, cc);
-    };
     F2 phi01, pi01, phi23, pi23;
-    pair(c01, f2_pack(um.x, um.y), f2_pack(up.x, up.y), f2_pack(im.x, im.y), f2_pack(ip.x, ip.y), km01, mid,
-         f2_pack(pv.x, pv.y), phi01, pi01);
-    pair(c23, f2_pack(um.z, um.w), f2_pack(up.z, up.w), f2_pack(im.z, im.w), f2_pack(ip.z, ip.w), mid, kp23,
-         f2_pack(pv.z, pv.w), phi23, pi23);
+    upd_pair(K, c01, f2_pack(um.x, um.y), f2_pack(up.x, up.y), f2_pack(im.x, im.y), f2_pack(ip.x, ip.y), km01, mid,
+             f2_pack(pv.x, pv.y), phi01, pi01);
+    upd_pair(K, c23, f2_pack(um.z, um.w), f2_pack(up.z, up.w), f2_pack(im.z, im.w), f2_pack(ip.z, ip.w), mid, kp23,
+             f2_pack(pv.z, pv.w), phi23, pi23);
     phi_n = make_float4(f2_lo(phi01), f2_hi(phi01), f2_lo(phi23), f2_hi(phi23));
     pi_n = make_float4(f2_lo(pi01), f2_hi(pi01), f2_lo(pi23), f2_hi(pi23));
 }
+
+/* The halo rows' share of a thread: HW consecutive sites of a row (HW = 1, 2
+ * or 4), as float, float2 or float4, with shared-memory loads and stores of
+ * that width, and the update of those sites (the same packed pairs). */
+template <int HW>
+struct Hv;
+template <>
+struct Hv<4> {
+    using T = float4;
+    static __device__ __forceinline__ T ld(uint32_t a) { return lds4(a); }
+    static __device__ __forceinline__ void st(uint32_t a, const T &v) { sts4(a, v); }
+    static __device__ __forceinline__ float first(const T &v) { return v.x; }
+    static __device__ __forceinline__ float last(const T &v) { return v.w; }
+    static __device__ __forceinline__ void update(const Pk &K, const T &c, const T &um, const T &up, const T &im,
+                                                  const T &ip, float left, float right, const T &pv, T &phi, T &pi) {
+        update4(K, c, um, up, im, ip, left, right, pv, phi, pi);
+    }
+};
+template <>
+struct Hv<2> {
+    using T = float2;
+    static __device__ __forceinline__ T ld(uint32_t a) {
+        float2 v;
+        asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+        return v;
+    }
+    static __device__ __forceinline__ void st(uint32_t a, const T &v) {
+        asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.x), "f"(v.y) : "memory");
+    }
+    static __device__ __forceinline__ float first(const T &v) { return v.x; }
+    static __device__ __forceinline__ float last(const T &v) { return v.y; }
+    static __device__ __forceinline__ void update(const Pk &K, const T &c, const T &um, const T &up, const T &im,
+                                                  const T &ip, float left, float right, const T &pv, T &phi, T &pi) {
+        F2 p2, q2;
+        upd_pair(K, f2_pack(c.x, c.y), f2_pack(um.x, um.y), f2_pack(up.x, up.y), f2_pack(im.x, im.y),
+                 f2_pack(ip.x, ip.y), f2_pack(left, c.x), f2_pack(c.y, right), f2_pack(pv.x, pv.y), p2, q2);
+        phi = make_float2(f2_lo(p2), f2_hi(p2));
+        pi = make_float2(f2_lo(q2), f2_hi(q2));
+    }
+};
+template <>
+struct Hv<1> {
+    using T = float;
+    static __device__ __forceinline__ T ld(uint32_t a) {
+        float v;
+        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+        return v;
+    }
+    static __device__ __forceinline__ void st(uint32_t a, const T &v) {
+        asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+    }
+    static __device__ __forceinline__ float first(const T &v) { return v; }
+    static __device__ __forceinline__ float last(const T &v) { return v; }
+    /* one site: both halves of the pair carry it (each half is rounded on its own) */
+    static __device__ __forceinline__ void update(const Pk &K, const T &c, const T &um, const T &up, const T &im,
+                                                  const T &ip, float left, float right, const T &pv, T &phi, T &pi) {
+        F2 p2, q2;
+        upd_pair(K, f2_splat(c), f2_splat(um), f2_splat(up), f2_splat(im), f2_splat(ip), f2_splat(left),
+                 f2_splat(right), f2_splat(pv), p2, q2);
+        phi = f2_lo(p2);
+        pi = f2_lo(q2);
+    }
+};
 
 /* A tile position of a thread (row r1 of the level-1 rows j0 - 1 .. j0 + tj,
  * vector kv of the row), updated at both levels in every plane of an item,
@@ -117,18 +184,17 @@ __device__ __forceinline__ void update4(const Pk &K, const float4 c, const float
  *             m + 1 from the stage that just landed);
  *   y_m, y_c, y_p  level-1 phi at planes m' - 1, m', m' + 1 (level 2 at m');
  *   z, zz     level-1 pi at planes m', m' + 1.
- * A halo position (rows j0 - 1, j0 + tj) is updated at level 1 only and
- * keeps only x_m, x_c. */
+ * The halo rows (j0 - 1, j0 + tj) are updated at level 1 only; a thread's
+ * share of them keeps only x_m, x_c. */
 struct Slot {
     float4 x_m, x_c, y_m, y_c, y_p, z, zz;
 };
-struct HSlot {
-    float4 x_m, x_c;
-};
 
 /* Two leapfrog steps per pass (see the file comment). Thread c owns the tile
- * positions c and NT + c (NT = tile positions / 2 = threads) and, for
- * c < 2 n / 4, halo position c (row j0 - 1, then row j0 + tj). Rows hold a
+ * positions c and NT + c (NT = tile positions / 2 = threads) and HW sites of
+ * the halo rows (row j0 - 1, then row j0 + tj), sites HW c .. HW c + HW - 1:
+ * HW = 2 n / NT (1 or 2) gives every thread the same share; HW = 4 gives
+ * threads c < 2 n / 4 one vector each (where 2 n / NT is not 1 or 2). Rows hold a
  * multiple of 32 vectors, so a warp's 32 positions of a slot are 32
  * consecutive vectors of one row: the axis-2 neighbours come from the next
  * lanes by shuffle (the end lanes read them from shared memory), and the
@@ -141,6 +207,7 @@ struct HSlot {
  * ends with one barrier of all threads; plane g's stage is free once round
  * g + 1 has ended, so at the start of round g thread 0 issues the copies of
  * planes up to g + nstage - 2 (no other wait). */
+template <int HW>
 __global__ void __launch_bounds__(TB_MAXT, 1)
     k_step3_t2(StepConst k, int tj, int nstage, int parts, const float *__restrict__ phi_in,
                const float *__restrict__ pi_in, float *__restrict__ phi_out, float *__restrict__ pi_out,
@@ -241,13 +308,15 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
     K.nc2 = f2_splat(-k.c2f);
     K.c3 = f2_splat(k.c3f);
     K.nc4 = f2_splat(-k.c4f);
-    const int nvr = n / W;                     /* vectors per row (a multiple of 32) */
     /* the positions as offsets r1 n + kk in an array of level-1 rows (row r1,
      * first site kk; rows hold n = W nvr sites, so tile position u sits at
      * n + W u): tile slot s at off0 + s W NT, the halo slot at offh */
     const int off0 = n + W * threadIdx.x, slot_step = W * NT;
-    const bool has_h = threadIdx.x < 2 * nvr;
-    const int offh = W * threadIdx.x + (threadIdx.x < nvr ? 0 : tj * n);
+    using H = Hv<HW>;
+    using HT = typename H::T;
+    const bool has_h = HW * (int)threadIdx.x < 2 * n;
+    const int fh = HW * threadIdx.x;                        /* first halo site, counted over both rows */
+    const int offh = fh + (fh < n ? 0 : tj * n);
     const uint32_t first_lane = lane == 0, last_lane = lane == 31;
     /* every slot of a thread starts at the same site of its row (the slots are
      * whole rows apart: tj is even), kk = W threadIdx.x mod n; the periodic
@@ -257,6 +326,9 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
     /* the axis-2 neighbours of the vector at shared byte address a: from the
      * neighbouring lanes, the warp's end lanes from the row */
     const int ladj_b = 4 * (ladj - 1), radj_b = 4 * (radj + W);
+    /* the same for the halo share (first site kk_h of its row, HW sites) */
+    const int kk_h = fh % n;
+    const int ladjh_b = 4 * ((kk_h == 0 ? n : 0) - 1), radjh_b = 4 * ((kk_h + HW == n ? -n : 0) + HW);
     auto sides = [&](const float4 &c, uint32_t a, float &left, float &right) {
         left = __shfl_up_sync(0xffffffffu, c.w, 1);
         right = __shfl_down_sync(0xffffffffu, c.x, 1);
@@ -291,7 +363,7 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
         return any_bad;
     };
     Slot sl[TB_NTS];
-    HSlot hs;
+    HT hxm, hxc;
     long long g = 0;     /* the round: index of the input plane it waits for */
     bool bad = false;
     for (int j = 0;; ++j) {
@@ -305,7 +377,7 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
             const uint32_t S = ring_a + gs * stage_b + nb;
 #pragma unroll
             for (int s = 0; s < TB_NTS; ++s) sl[s].x_m = lds4(S + 4u * (off0 + s * slot_step));
-            if (has_h) hs.x_m = lds4(S + 4u * offh);
+            if (has_h) hxm = H::ld(S + 4u * offh);
         } else {
             bad = true;
         }
@@ -316,7 +388,7 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
             const uint32_t S = ring_a + gs * stage_b + nb;
 #pragma unroll
             for (int s = 0; s < TB_NTS; ++s) sl[s].x_c = lds4(S + 4u * (off0 + s * slot_step));
-            if (has_h) hs.x_c = lds4(S + 4u * offh);
+            if (has_h) hxc = H::ld(S + 4u * offh);
         } else {
             bad = true;
         }
@@ -376,8 +448,22 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
                     if (m2 >= p0) level2(x, off);
                 }
                 if (has_h) {
-                    float4 phi1, pi1;
-                    level1(hs.x_m, hs.x_c, offh, phi1, pi1);
+                    /* level 1 at plane q - 1 on the halo share */
+                    const uint32_t ob = 4u * (uint32_t)offh;
+                    const HT xp = H::ld(Sn + nb + ob);
+                    const HT um = H::ld(S0 + ob);
+                    const HT up = H::ld(S0 + 2u * nb + ob);
+                    const HT pv = H::ld(S0 + pi_b + ob);
+                    const uint32_t a = S0 + nb + ob;
+                    float left = __shfl_up_sync(0xffffffffu, H::last(hxc), 1);
+                    float right = __shfl_down_sync(0xffffffffu, H::first(hxc), 1);
+                    lds1_if(left, a + ladjh_b, first_lane);
+                    lds1_if(right, a + radjh_b, last_lane);
+                    HT phi1, pi1;
+                    H::update(K, hxc, um, up, hxm, xp, left, right, pv, phi1, pi1);
+                    H::st(D1 + ob, phi1);
+                    hxm = hxc;
+                    hxc = xp;
                 }
             } else {
                 bad = true;
@@ -478,10 +564,13 @@ cudaError_t launch_step3_tb(int prec, const StepConst &k, int tl, const void *ph
     size_t smem;
     unsigned grid;
     if (!step3tb_geometry(k, prec, tl, tj, nstage, smem, grid, parts)) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(k_step3_t2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
     const int nc = step3tb_consumers(k.n, tj);
-    return launch_pdl(k_step3_t2, dim3(grid), dim3(nc), smem, s, k, tj, nstage, parts, (const float *)phi_in,
+    /* the halo rows' 2 n sites over all threads where that is 1 or 2 sites each */
+    const int hw = (2 * k.n) % nc == 0 ? 2 * k.n / nc : 4;
+    auto fn = hw == 1 ? k_step3_t2<1> : (hw == 2 ? k_step3_t2<2> : k_step3_t2<4>);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return launch_pdl(fn, dim3(grid), dim3(nc), smem, s, k, tj, nstage, parts, (const float *)phi_in,
                       (const float *)pi_in, (float *)phi_out, (float *)pi_out, st);
 }
 
