@@ -244,7 +244,11 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
     /* ---- the copies (thread 0): planes are issued in stream order; the
      *      producer's item j is published in item_q[j % TB_IQ] before its
      *      first plane is issued ---- */
-    int pr_j = 0, pr_it = -1, pr_pl = 0, pr_p1 = 0, pr_j0 = 0;   /* producer: item, next plane */
+    int pr_j = 0, pr_it = -1, pr_pl = 0, pr_p1 = 0;              /* producer: item, next plane */
+    /* the item's source rows (periodic), as element offsets within a plane:
+     * phi rows j0 - 2, j0 - 1, j0 .. j0 + tj - 1, j0 + tj, j0 + tj + 1; pi rows
+     * j0 - 1, j0 .. j0 + tj - 1, j0 + tj */
+    __shared__ size_t pr_r[6];   /* thread 0's only: kept out of the registers */
     long long issued = 0;                                        /* planes issued so far */
     int is_stage = 0;                                            /* its stage: issued mod nstage */
     bool pr_done = false;
@@ -261,7 +265,9 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
         item_of(pr_it, t, p0, p1);
         pr_pl = p0 - 2;
         pr_p1 = p1;
-        pr_j0 = t * tj;
+        const int j0 = t * tj;
+        const int rows[6] = {(j0 - 2 + n) % n, (j0 - 1 + n) % n, j0, (j0 + tj) % n, (j0 + tj + 1) % n, 0};
+        for (int e = 0; e < 6; ++e) pr_r[e] = (size_t)rows[e] * n;
     };
     auto issue_upto = [&](long long last) {
         while (!pr_done && issued <= last) {
@@ -271,18 +277,17 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
             float *dpi = dst + (size_t)R0 * n;
             const float *gphi = phi_in + (size_t)pw * plane;
             const float *gpi = pi_in + (size_t)pw * plane;
-            const int j0 = pr_j0;
+            const uint32_t rb = (uint32_t)row_bytes;
             fence_proxy_async();
             mbar_arrive_expect_tx(&full[s], tx_bytes);
-            for (int e = 0; e < 2; ++e) {
-                const int ra = (j0 - 2 + e + n) % n, rb = (j0 + tj + e) % n;
-                bulk_g2s(dst + (size_t)e * n, gphi + (size_t)ra * n, (uint32_t)row_bytes, &full[s]);
-                bulk_g2s(dst + (size_t)(2 + tj + e) * n, gphi + (size_t)rb * n, (uint32_t)row_bytes, &full[s]);
-            }
-            bulk_g2s(dst + (size_t)2 * n, gphi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
-            bulk_g2s(dpi, gpi + (size_t)((j0 - 1 + n) % n) * n, (uint32_t)row_bytes, &full[s]);
-            bulk_g2s(dpi + n, gpi + (size_t)j0 * n, (uint32_t)(tj * row_bytes), &full[s]);
-            bulk_g2s(dpi + (size_t)(1 + tj) * n, gpi + (size_t)((j0 + tj) % n) * n, (uint32_t)row_bytes, &full[s]);
+            bulk_g2s(dst, gphi + pr_r[0], rb, &full[s]);
+            bulk_g2s(dst + n, gphi + pr_r[1], rb, &full[s]);
+            bulk_g2s(dst + (size_t)2 * n, gphi + pr_r[2], (uint32_t)tj * rb, &full[s]);
+            bulk_g2s(dst + (size_t)(2 + tj) * n, gphi + pr_r[3], rb, &full[s]);
+            bulk_g2s(dst + (size_t)(3 + tj) * n, gphi + pr_r[4], rb, &full[s]);
+            bulk_g2s(dpi, gpi + pr_r[1], rb, &full[s]);
+            bulk_g2s(dpi + n, gpi + pr_r[2], (uint32_t)tj * rb, &full[s]);
+            bulk_g2s(dpi + (size_t)(1 + tj) * n, gpi + pr_r[3], rb, &full[s]);
             ++issued;
             if (++is_stage == nstage) is_stage = 0;
             if (++pr_pl > pr_p1 + 1) next_item();
