@@ -232,12 +232,14 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         const int nvec = tj * nvec_row;
         const int row_step = NC / nvec_row, vec_step = NC % nvec_row;
         constexpr bool want_eg = SUMS == SUM_FULL || SUMS == SUM_FRIEDMANN_EG;
-        constexpr bool PACKED = std::is_same<T, float>::value && (SUMS == SUM_NONE || SUMS == SUM_FRIEDMANN);
+        /* float steps run in packed f32x2 pairs, with or without sums */
+        constexpr bool PACKED = std::is_same<T, float>::value;
         /* packed-pair constants of the f32x2 path (unused otherwise) */
         const F2 P_FL = f2_splat((float)fl), P_IDX2 = f2_splat((float)inv_dx2), P_NFV = f2_splat(-(float)fv);
         const F2 P_DT = f2_splat((float)dt), P_KW = f2_splat((float)kin_w);
         const F2 P_C2 = f2_splat(k.c2f), P_NC3 = f2_splat(-k.c3f), P_C4 = f2_splat(k.c4f);
         const F2 P_V2 = f2_splat(k.v2f), P_NV3 = f2_splat(-k.v3f), P_V4 = f2_splat(k.v4f), P_DV = f2_splat(k.dvf);
+        const F2 P_IADX = f2_splat((float)inv_adx), P_VW = f2_splat((float)vel_w), P_HALF = f2_splat(0.5f);
         /* wait for the ring position under cursor c to land */
         auto acquire = [&](const Cursor &c) -> bool {
             const bool ok = abort_flag == 0 && mbar_wait(&full[c.s], c.ph, WAIT_LIMIT);
@@ -354,16 +356,19 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                     const int ro = (r + 1) * n + (kk + W == n ? 0 : kk + W);
                     const T left = S0[lo];
                     const T right = S0[ro];
-                    VT phi_new, pi_new, vek, veg, vep;
+                    VT phi_new, pi_new, vek{}, veg{}, vep{};
                     if constexpr (PACKED) {
-                    /* float, no sums or the Friedmann sums only: the four sites as two
-                     * packed pairs (f32x2 arithmetic, one instruction per pair), the
-                     * same operations in the same order as the scalar path */
+                    /* float: the four sites as two packed pairs (f32x2 arithmetic, one
+                     * instruction per pair), the same operations in the same order as
+                     * the scalar path for the fields; the sums of a pair's two sites
+                     * are added pairwise over the vector, then its sum enters the
+                     * compensated per-thread accumulator */
                     const F2 c01 = f2_pack(c.x, c.y), c23 = f2_pack(c.z, c.w);
                     const F2 km01 = f2_pack(left, c.x), mid = f2_pack(c.y, c.z), kp23 = f2_pack(c.w, right);
-                    F2 phi01, pi01, phi23, pi23, ek01, ek23, ep01, ep23;
+                    F2 phi01, pi01, phi23, pi23;
+                    F2 v01[NS], v23[NS];   /* the pair's terms of the sums (S_EK, S_EP, S_EG first) */
                     auto pair = [&](F2 cc, F2 umm, F2 upp, F2 imm, F2 ipp, F2 kmm, F2 kpp, F2 pp, F2 &phi_n,
-                                    F2 &pi_n, F2 &ek, F2 &ep) {
+                                    F2 &pi_n, F2 (&v)[NS]) {
                         const F2 two = f2_add(cc, cc);
                         const F2 t0 = f2_add(f2_sub(ipp, two), imm);
                         const F2 t1 = f2_add(f2_sub(upp, two), umm);
@@ -374,22 +379,55 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                         const F2 force = f2_fma(f2_mul(P_FL, lap), P_IDX2, f2_mul(P_NFV, f2_mul(cc, h)));
                         pi_n = f2_fma(P_DT, force, pp);
                         phi_n = DF ? cc : f2_fma(P_DT, pi_n, cc);
-                        if constexpr (SUMS == SUM_FRIEDMANN) {
-                            ek = f2_mul(f2_mul(P_KW, pi_n), pi_n);
+                        if constexpr (SUMS != SUM_NONE) {
+                            /* kinetic (bubble.cpp:810) and potential (808) energy */
+                            const F2 ek = f2_mul(f2_mul(P_KW, pi_n), pi_n);
                             /* V(f) = DeltaV + f^2 (v2 + f (-v3 + f v4)) */
-                            ep = f2_fma(f2_mul(cc, cc), f2_fma(cc, f2_fma(cc, P_V4, P_NV3), P_V2), P_DV);
+                            const F2 ep = f2_fma(f2_mul(cc, cc), f2_fma(cc, f2_fma(cc, P_V4, P_NV3), P_V2), P_DV);
+                            v[S_EK] = ek;
+                            v[S_EP] = ep;
+                            F2 eg = f2_splat(0.f);
+                            if constexpr (want_eg) {
+                                /* forward gradients: x <- axis 1, y <- axis 0, z <- axis 2 (bubble.cpp:794-801) */
+                                const F2 gx = f2_mul(f2_sub(upp, cc), P_IADX);
+                                const F2 gy = f2_mul(f2_sub(ipp, cc), P_IADX);
+                                const F2 gz = f2_mul(f2_sub(kpp, cc), P_IADX);
+                                eg = f2_mul(P_HALF, f2_add(f2_add(f2_mul(gx, gx), f2_mul(gy, gy)), f2_mul(gz, gz)));
+                                v[S_EG] = eg;
+                            }
+                            if constexpr (SUMS == SUM_FULL) {
+                                const F2 vv = f2_mul(pi_n, P_VW);
+                                const F2 et = f2_add(f2_add(ek, eg), ep);
+                                v[S_PHI] = cc;
+                                v[S_V] = vv;
+                                v[Q_EK] = f2_mul(ek, ek);
+                                v[Q_EP] = f2_mul(ep, ep);
+                                v[Q_EG] = f2_mul(eg, eg);
+                                v[Q_ET] = f2_mul(et, et);
+                                v[Q_PHI] = f2_mul(cc, cc);
+                                v[Q_V] = f2_mul(vv, vv);
+                                v[S_EKIN_IN] = f2_mul(f2_mul(P_KW, pp), pp);
+                            }
                         }
                     };
                     pair(c01, f2_pack(um.x, um.y), f2_pack(up.x, up.y), f2_pack(im.x, im.y), f2_pack(ip.x, ip.y),
-                         km01, mid, f2_pack(pv.x, pv.y), phi01, pi01, ek01, ep01);
+                         km01, mid, f2_pack(pv.x, pv.y), phi01, pi01, v01);
                     pair(c23, f2_pack(um.z, um.w), f2_pack(up.z, up.w), f2_pack(im.z, im.w), f2_pack(ip.z, ip.w),
-                         mid, kp23, f2_pack(pv.z, pv.w), phi23, pi23, ek23, ep23);
+                         mid, kp23, f2_pack(pv.z, pv.w), phi23, pi23, v23);
                     phi_new = make_float4(f2_lo(phi01), f2_hi(phi01), f2_lo(phi23), f2_hi(phi23));
                     pi_new = make_float4(f2_lo(pi01), f2_hi(pi01), f2_lo(pi23), f2_hi(pi23));
-                    if constexpr (SUMS == SUM_FRIEDMANN) {
-                        const F2 ek = f2_add(ek01, ek23), ep = f2_add(ep01, ep23);
-                        acc[S_EK].add(f2_lo(ek) + f2_hi(ek));
-                        acc[S_EP].add(f2_lo(ep) + f2_hi(ep));
+                    if constexpr (SUMS != SUM_NONE) {
+                        constexpr int NA = SUMS == SUM_FULL ? NSUM : (want_eg ? 3 : 2);
+#pragma unroll
+                        for (int q = 0; q < NA; ++q) {
+                            const F2 t = f2_add(v01[q], v23[q]);
+                            acc[q].add(f2_lo(t) + f2_hi(t));
+                        }
+                        if constexpr (SUMS == SUM_FULL) {
+                            vek = make_float4(f2_lo(v01[S_EK]), f2_hi(v01[S_EK]), f2_lo(v23[S_EK]), f2_hi(v23[S_EK]));
+                            veg = make_float4(f2_lo(v01[S_EG]), f2_hi(v01[S_EG]), f2_lo(v23[S_EG]), f2_hi(v23[S_EG]));
+                            vep = make_float4(f2_lo(v01[S_EP]), f2_hi(v01[S_EP]), f2_lo(v23[S_EP]), f2_hi(v23[S_EP]));
+                        }
                     }
                     } else {
                     /* float: the sites of a vector are summed plainly (W terms), then
