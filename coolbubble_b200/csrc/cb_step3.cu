@@ -149,6 +149,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
     pdl_wait();          /* the previous step's fields, device state and work queue */
 
     Acc<T> acc[NSUM];
+    F2 pacc[NSUM];   /* float path: plain pair sums (the sums that are not compensated) */
 
     if (warp == CW) {
         /* ---- producer warp: lane 0 takes items from the queue and issues the
@@ -239,7 +240,8 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         const F2 P_DT = f2_splat((float)dt), P_KW = f2_splat((float)kin_w);
         const F2 P_C2 = f2_splat(k.c2f), P_NC3 = f2_splat(-k.c3f), P_C4 = f2_splat(k.c4f);
         const F2 P_V2 = f2_splat(k.v2f), P_NV3 = f2_splat(-k.v3f), P_V4 = f2_splat(k.v4f), P_DV = f2_splat(k.dvf);
-        const F2 P_IADX = f2_splat((float)inv_adx), P_VW = f2_splat((float)vel_w), P_HALF = f2_splat(0.5f);
+        /* gradient energy 0.5 |grad phi|^2 / (a dx)^2 as one product with the sum of squared differences */
+        const F2 P_EG = f2_splat((float)(0.5 * (double)inv_adx * (double)inv_adx)), P_VW = f2_splat((float)vel_w);
         /* wait for the ring position under cursor c to land */
         auto acquire = [&](const Cursor &c) -> bool {
             const bool ok = abort_flag == 0 && mbar_wait(&full[c.s], c.ph, WAIT_LIMIT);
@@ -303,7 +305,10 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
             const int j0 = t * tj;
             if (SUMS != SUM_NONE) {
 #pragma unroll
-                for (int s = 0; s < NSUM; ++s) acc[s] = Acc<T>{};
+                for (int s = 0; s < NSUM; ++s) {
+                    acc[s] = Acc<T>{};
+                    pacc[s] = f2_splat(0.f);
+                }
             }
             /* cm, c0, cp: cursors of planes i - 1, i, i + 1 */
             Cursor cm = cq, c0 = cq;
@@ -388,11 +393,9 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                             v[S_EP] = ep;
                             F2 eg = f2_splat(0.f);
                             if constexpr (want_eg) {
-                                /* forward gradients: x <- axis 1, y <- axis 0, z <- axis 2 (bubble.cpp:794-801) */
-                                const F2 gx = f2_mul(f2_sub(upp, cc), P_IADX);
-                                const F2 gy = f2_mul(f2_sub(ipp, cc), P_IADX);
-                                const F2 gz = f2_mul(f2_sub(kpp, cc), P_IADX);
-                                eg = f2_mul(P_HALF, f2_add(f2_add(f2_mul(gx, gx), f2_mul(gy, gy)), f2_mul(gz, gz)));
+                                /* forward differences: x <- axis 1, y <- axis 0, z <- axis 2 (bubble.cpp:794-801) */
+                                const F2 gx = f2_sub(upp, cc), gy = f2_sub(ipp, cc), gz = f2_sub(kpp, cc);
+                                eg = f2_mul(P_EG, f2_fma(gz, gz, f2_fma(gy, gy, f2_mul(gx, gx))));
                                 v[S_EG] = eg;
                             }
                             if constexpr (SUMS == SUM_FULL) {
@@ -404,7 +407,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                                 v[Q_EP] = f2_mul(ep, ep);
                                 v[Q_EG] = f2_mul(eg, eg);
                                 v[Q_ET] = f2_mul(et, et);
-                                v[Q_PHI] = f2_mul(cc, cc);
+                                v[Q_PHI] = f2_mul(cc, cc);   /* the same product as in V(f) */
                                 v[Q_V] = f2_mul(vv, vv);
                                 v[S_EKIN_IN] = f2_mul(f2_mul(P_KW, pp), pp);
                             }
@@ -421,7 +424,14 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
 #pragma unroll
                         for (int q = 0; q < NA; ++q) {
                             const F2 t = f2_add(v01[q], v23[q]);
-                            acc[q].add(f2_lo(t) + f2_hi(t));
+                            /* the energies (and the previous half step's kinetic sum, which
+                             * enters the time-centred Ekin) are compensated; the field
+                             * averages and the sums of squares behind the spreads are plain
+                             * float sums of pairs over the item's vectors (a few dozen per
+                             * thread at 512^3, restarted with every item: relative error
+                             * ~1e-6) */
+                            if (q == S_EK || q == S_EP || q == S_EG || q == S_EKIN_IN) acc[q].add(f2_lo(t) + f2_hi(t));
+                            else pacc[q] = f2_add(pacc[q], t);
                         }
                         if constexpr (SUMS == SUM_FULL) {
                             vek = make_float4(f2_lo(v01[S_EK]), f2_hi(v01[S_EK]), f2_lo(v23[S_EK]), f2_hi(v23[S_EK]));
@@ -545,6 +555,8 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
 #pragma unroll
                 for (int s = 0; s < NS; ++s) {
                     double x = acc[s].value();
+                    if constexpr (std::is_same<T, float>::value)
+                        x = __dadd_rn(x, __dadd_rn((double)f2_lo(pacc[s]), (double)f2_hi(pacc[s])));
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));
                     if (lane == 0) item_red[j & 1][warp][s] = x;
