@@ -28,6 +28,7 @@
  */
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cstdlib>
@@ -651,7 +652,7 @@ int sm_count() {
  * against the part-filled last round.
  * CB_STEP3_PARTS overrides the parts. */
 bool step3_geometry_parts(const StepConst &k, int prec, int &tj, int &nstage, size_t &smem, unsigned &grid,
-                          int &parts) {
+                          int &parts, bool whole_rounds = false) {
     if (k.d != 3) return false;
     const int n = k.n;
     const int esz = prec == P_FP64 ? 8 : 4;
@@ -700,7 +701,11 @@ bool step3_geometry_parts(const StepConst &k, int prec, int &tj, int &nstage, si
     for (int P = 1; P <= n / 4; ++P) {
         const double per_item = (double)n / P + fixed;
         const long long nitems = ntiles * P;
-        const double cost = nitems <= slots ? per_item : (double)nitems / slots * per_item + 0.5 * per_item;
+        /* whole_rounds (the full-sums step, issue-bound): every slot runs whole
+         * items, so a part-filled last round costs a whole item */
+        const double cost = whole_rounds ? (double)((nitems + slots - 1) / slots) * per_item
+                            : nitems <= slots ? per_item
+                                              : (double)nitems / slots * per_item + 0.5 * per_item;
         if (cost < best - 1e-9) {
             best = cost;
             parts = P;
@@ -718,13 +723,15 @@ bool step3_geometry(const StepConst &k, int prec, int &tj, int &nstage, size_t &
     return step3_geometry_parts(k, prec, tj, nstage, smem, grid, parts);
 }
 
-/* Rows of partial sums the staged kernel writes: one per work item. */
+/* Rows of partial sums the staged kernel writes: one per work item (the
+ * full-sums step of a static background may split the planes differently). */
 size_t step3_partial_rows(const StepConst &k, int prec) {
-    int tj, nstage, parts;
+    int tj, nstage, parts, parts_full;
     size_t smem;
     unsigned grid;
     if (!step3_geometry_parts(k, prec, tj, nstage, smem, grid, parts)) return 0;
-    return (size_t)(k.n / tj) * parts;
+    if (!step3_geometry_parts(k, prec, tj, nstage, smem, grid, parts_full, true)) return 0;
+    return (size_t)(k.n / tj) * (size_t)std::max(parts, parts_full);
 }
 
 cudaError_t launch_step3(int prec, const StepConst &k, bool df, int sums, const void *phi_in, const void *pi_in,
@@ -733,7 +740,8 @@ cudaError_t launch_step3(int prec, const StepConst &k, bool df, int sums, const 
     int tj, nstage, parts;
     size_t smem;
     unsigned grid;
-    if (!step3_geometry_parts(k, prec, tj, nstage, smem, grid, parts)) return cudaErrorInvalidValue;
+    if (!step3_geometry_parts(k, prec, tj, nstage, smem, grid, parts, sums == SUM_FULL && !df))
+        return cudaErrorInvalidValue;
 #define CB_LAUNCH3(T, DFv, SU)                                                                                     \
     do {                                                                                                           \
         auto fn = k_step3<T, DFv, SU>;                                                                             \
