@@ -15,7 +15,12 @@
  *   columns : every leading axis, in place, on tiles of C contiguous
  *             columns (C * 16 B coalesced segments per row of the tile).
  *   bins    : one pass over the half-complex array; per-block shared-memory
- *             histograms, then a fixed-order sum over blocks (deterministic).
+ *             histograms, then a fixed-order sum over the blocks' histograms.
+ * For d = 2, 3 and n a power of two from 64 to 512 (the spectrum of every
+ * benchmark lattice) the forward transform runs instead on register-resident
+ * kernels (k_fft_rows_reg, k_fft_cols_reg; same stages, same twiddles, same
+ * results), and the spectrum bins inside the last column pass, which then
+ * writes nothing back: three passes over the data instead of five.
  */
 #include <cuda_runtime.h>
 
@@ -37,7 +42,10 @@ struct FftState {
     double *bins_out = nullptr; /* 3 * nbins */
     int hist_blocks = 0;
     int nbins = 0;
-    size_t half_elems = 0;
+    int pitch = 0;            /* complex values per row of half (n/2+1, or rounded up to 8) */
+    bool reg = false;         /* forward transforms by the register-resident kernels */
+    bool geom_done = false;   /* bins_out holds the mode counts and k sums (register path) */
+    size_t half_elems = 0;    /* rows * pitch */
 };
 
 namespace {
@@ -333,13 +341,297 @@ __global__ void __launch_bounds__(FFT_T) k_fft_rows_c2r(Plan pl, const double2 *
     }
 }
 
+/* ---- Register-resident forward transforms for n = 2^k, 64 <= n <= 512 ----
+ *
+ * A sequence of length n is held by n/8 threads, eight elements each: thread
+ * j holds elements j + m n/8 (m < 8) before every stage, and the stages are
+ * the same Stockham stages as above (radix 8, then one radix 4 or 2), done in
+ * registers; between two stages the outputs go through shared memory once
+ * (two buffers used in turn: one barrier per exchange). The first stage reads
+ * its inputs straight from global memory and the last stage leaves the
+ * outputs in natural order (thread j: X_{j + m n/8}), so a length-512
+ * transform costs two shared-memory exchanges instead of three stage passes
+ * plus a load and a store pass. Blocks are persistent (one per resident slot)
+ * and load the next tile into registers before transforming the current one,
+ * so the loads overlap the arithmetic. The arithmetic is that of the
+ * shared-memory kernels: the same radices in the same order, the same twiddle
+ * table, hence bit-identical results.
+ *
+ * The half-complex array has a row pitch of n/2 + 1 rounded up to 8 complex
+ * values (128 bytes), so every 8-column tile of a column pass reads and writes
+ * whole 128-byte lines. */
+/* Sequences (columns, or row pairs) per tile: 8 up to n = 256, 4 at n = 512,
+ * so that a block has at most 256 threads and two blocks share an SM (a block
+ * at its barrier then leaves the SM to the other). */
+constexpr int PITCH_ALIGN = 8;   /* complex values per 128-byte line */
+__host__ __device__ constexpr int rc_of(int n) { return n <= 256 ? 8 : 4; }
+
+/* Radix of the stage after earlier radices with product NS, in a length-N
+ * plan: 8 while 8 divides what is left, then the remaining 4 or 2 (the order
+ * factor() gives). */
+__host__ __device__ constexpr int radix_of(int N, int NS) { return (N / NS) % 8 == 0 ? 8 : N / NS; }
+__host__ __device__ constexpr int lg2c(int x) { return x <= 1 ? 0 : 1 + lg2c(x / 2); }
+
+/* One stage on the thread's eight elements: U = 8 / R butterflies, butterfly
+ * u takes elements u + r U (its inputs j + u N/8 + r N/R). */
+template <int R, int N, int NS>
+__device__ __forceinline__ void rstage(double2 (&v)[8], int j, const double2 *__restrict__ tw) {
+    constexpr int U = 8 / R, N8 = N / 8, TWS = N / (NS * R);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int jm = (j + u * N8) & (NS - 1);
+        double2 x[MAX_RADIX];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            double2 y = v[u + r * U];
+            if (NS > 1 && r && jm) y = cmul(y, __ldg(&tw[r * jm * TWS]));
+            x[r] = y;
+        }
+        dft_small<R>(x, tw, N);
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[u + r * U] = x[r];
+    }
+}
+
+/* The stage's outputs to shared memory at their Stockham places
+ * (b / NS) NS R + b mod NS + r NS of butterfly b = j + u N/8. */
+template <int R, int N, int NS, class Lay>
+__device__ __forceinline__ void rput(double2 *buf, const double2 (&v)[8], int j, Lay lay) {
+    constexpr int U = 8 / R, N8 = N / 8, LG = lg2c(NS);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int b = j + u * N8;
+        const int base = ((b >> LG) << LG) * R + (b & (NS - 1));
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[lay(base + r * NS)] = v[u + r * U];
+    }
+}
+
+/* The stages from the one after radices with product NS; sb0 / sb1 are the
+ * exchange buffers, par the next one to use (kept across calls: a buffer is
+ * rewritten only after a barrier that every thread passes after its last
+ * read of it). */
+template <int N, int NS, class Lay>
+__device__ __forceinline__ void fft_stages(double2 (&v)[8], int j, const double2 *__restrict__ tw, double2 *sb0,
+                                           double2 *sb1, int &par, Lay lay) {
+    if constexpr (NS < N) {
+        constexpr int R = radix_of(N, NS);
+        rstage<R, N, NS>(v, j, tw);
+        if constexpr (NS * R < N) {
+            double2 *buf = par ? sb1 : sb0;
+            par ^= 1;
+            rput<R, N, NS>(buf, v, j, lay);
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < 8; ++m) v[m] = buf[lay(j + m * (N / 8))];
+        }
+        fft_stages<N, NS * R>(v, j, tw, sb0, sb1, par, lay);
+    }
+}
+
+/* Column tiles: element (index, column c) at index * RC + c; with 4 columns
+ * one pad slot per two indices (no bank conflicts in either case). */
+template <int RC>
+struct ColLay {
+    __device__ __forceinline__ int operator()(int idx) const {
+        return RC == 8 ? idx * RC + c : idx * RC + c + (idx >> 1);
+    }
+    int c;
+};
+/* complex values of one exchange buffer of a column tile */
+__host__ __device__ constexpr int col_buf(int n, int rc) { return rc == 8 ? n * rc : n * rc + n / 2; }
+/* Row-pair tiles: sequence c at c (n + n/8), one pad slot per 8 elements. */
+struct RowLay {
+    __device__ __forceinline__ int operator()(int idx) const { return base + idx + (idx >> 3); }
+    int base;
+};
+
+/* Last axis, forward, persistent: tile g = row pairs 8 g .. 8 g + 7 (rows
+ * 16 g .. 16 g + 15); thread (j, c) = (tid mod n/8, tid / n/8). The two real
+ * rows of a pair are transformed as one complex sequence and separated after
+ * a last exchange, as in k_fft_rows. Needs rows a multiple of 16. */
+template <typename T, int N>
+__global__ void __launch_bounds__(256, 2) k_fft_rows_reg(const T *__restrict__ field, unsigned ntiles, int pitch,
+                                                        const double2 *__restrict__ tw, double2 *__restrict__ out) {
+    extern __shared__ double2 sm[];
+    constexpr int RC = rc_of(N), n = N, n8 = N / 8, h = N / 2 + 1, P = N + N / 8;
+    const int j = threadIdx.x % n8, c = threadIdx.x / n8;
+    double2 *sb0 = sm, *sb1 = sm + RC * P;
+    const RowLay lay{c * P};
+    int par = 0;
+    T xa[8], xb[8];
+    auto load = [&](unsigned g) {
+        const size_t ra = 2 * ((size_t)g * RC + c);
+        const T *pa = field + ra * n + j, *pb = pa + n;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            xa[m] = __ldg(pa + m * n8);
+            xb[m] = __ldg(pb + m * n8);
+        }
+    };
+    unsigned g = blockIdx.x;
+    if (g < ntiles) load(g);
+    for (; g < ntiles; g += gridDim.x) {
+        double2 v[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) v[m] = make_double2((double)xa[m], (double)xb[m]);
+        if (g + gridDim.x < ntiles) load(g + gridDim.x);
+        fft_stages<N, 1>(v, j, tw, sb0, sb1, par, lay);
+        /* Z in natural order to shared memory, then A_k, B_k for k <= n/2 */
+        double2 *buf = par ? sb1 : sb0;
+        par ^= 1;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) buf[lay(j + m * n8)] = v[m];
+        __syncthreads();
+        const size_t ra = 2 * ((size_t)g * RC + c);
+        double2 *oa = out + ra * pitch, *ob = oa + pitch;
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+            const int k = j + m * n8;
+            if (k < h) {
+                const double2 zk = buf[lay(k)];
+                const double2 zc = buf[lay(k == 0 ? 0 : n - k)];
+                /* A = (Z_k + conj Z_{n-k}) / 2, B = (Z_k - conj Z_{n-k}) / (2i) */
+                oa[k] = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y - zc.y));
+                ob[k] = make_double2(0.5 * (zk.y + zc.y), -0.5 * (zk.x - zc.x));
+            }
+        }
+    }
+}
+
+/* A leading axis, forward, persistent: the array is [outer][n][inner] (inner
+ * a multiple of RC); tile t = (o, RC consecutive columns); thread (j, c) =
+ * (tid / RC, tid mod RC). BINS = 0: the transform is written back in place.
+ * BINS = 1, 2 (the last axis of the spectrum, outer = 1): nothing is written
+ * back; the tile goes through shared memory once more and each thread bins
+ * 8 consecutive rows (k0) of one column like k_bins, adding into registers
+ * while the shell stays the same and into the block's shared histogram when
+ * it changes; the block's histogram goes to its own row of hist at the end.
+ * BINS = 2 bins the mode counts and the k sums as well; they depend only on
+ * the lattice, so a spectrum state computes them on its first call and later
+ * calls (BINS = 1) bin the power alone. */
 struct BinConst {
-    int d, n, h, nbins;
+    int d, n, h, pitch, nbins;
     size_t rows;
     double dk, pref, pnorm;
 };
 
 __device__ __forceinline__ long long sidx(long long i, int n) { return (i <= n / 2) ? i : i - n; }
+
+template <int BINS, int N>
+__global__ void __launch_bounds__(256, 2) k_fft_cols_reg(double2 *data, unsigned ntiles, size_t inner,
+                                                        const double2 *__restrict__ tw, BinConst bc, double *hist) {
+    extern __shared__ double2 sm[];
+    constexpr int RC = rc_of(N), n = N, n8 = N / 8;
+    const int j = threadIdx.x / RC, c = threadIdx.x % RC;
+    const int bp = col_buf(n, RC);   /* exchange buffer (the binning's transpose fits the same size) */
+    double2 *sb0 = sm, *sb1 = sm + bp;
+    double *hs = reinterpret_cast<double *>(sm + 2 * (size_t)bp);
+    double *pw = hs, *ws = hs + bc.nbins, *ks = hs + 2 * bc.nbins;
+    constexpr int NH = BINS == 2 ? 3 : 1;   /* histograms binned */
+    if (BINS) {
+        for (int i = threadIdx.x; i < NH * bc.nbins; i += blockDim.x) hs[i] = 0.0;
+        /* ordered before the first histogram add by the first exchange's barrier */
+    }
+    const ColLay<RC> lay{c};
+    const size_t tpo = inner / RC;   /* tiles per outer index */
+    int par = 0;
+    double2 nx[8];
+    auto at = [&](unsigned t) -> double2 * {
+        const size_t o = t / tpo, q = (t - o * tpo) * RC + c;
+        return data + o * (size_t)n * inner + q + (size_t)j * inner;
+    };
+    auto load = [&](unsigned t) {
+        const double2 *p = at(t);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) nx[m] = p[(size_t)m * n8 * inner];
+    };
+    unsigned t = blockIdx.x;
+    if (t < ntiles) load(t);
+    for (; t < ntiles; t += gridDim.x) {
+        double2 v[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) v[m] = nx[m];
+        if (t + gridDim.x < ntiles) load(t + gridDim.x);
+        fft_stages<N, 1>(v, j, tw, sb0, sb1, par, lay);
+        if constexpr (!BINS) {
+            double2 *p = at(t);
+#pragma unroll
+            for (int m = 0; m < 8; ++m) p[(size_t)m * n8 * inner] = v[m];
+        } else {
+            /* the tile in natural order (row k0, column c at tr(k0, c): no bank
+             * conflicts either way), then thread tid bins rows 8 (tid / RC) ..
+             * + 7 of column tid mod RC: along those rows the shell changes
+             * rarely, and the lanes of a warp cover 8 RC rows, so few of them
+             * add into the same shell at once */
+            auto tr = [&](int k0, int cc) { return k0 * RC + cc + (RC == 4 ? 4 * (k0 >> 3) : 0); };
+            double2 *buf = par ? sb1 : sb0;
+            par ^= 1;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) buf[tr(j + m * n8, c)] = v[m];
+            __syncthreads();
+            const int cc = threadIdx.x % RC, r0 = 8 * (threadIdx.x / RC);
+            const size_t q0 = (size_t)t * RC;   /* outer = 1 */
+            int k1 = 0, kz = (int)q0 + cc;
+            if (bc.d == 3) {
+                k1 = (int)(q0 / (size_t)bc.pitch);
+                kz = (int)(q0 - (size_t)k1 * bc.pitch) + cc;
+            }
+            if (kz < bc.h) {
+                const double s1 = bc.d == 3 ? (double)(k1 <= n / 2 ? k1 : k1 - n) : 0.0;
+                const double w = (kz == 0 || kz == n / 2) ? 1.0 : 2.0;
+                const double wp = __dmul_rn(w, bc.pref);
+                const double kz2 = (double)kz * (double)kz;
+                int cur = -1;
+                double ap = 0.0, aw = 0.0, ak = 0.0;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int k0 = r0 + i;
+                    const double s0 = (double)(k0 <= n / 2 ? k0 : k0 - n);
+                    const double n2rows = bc.d == 3 ? __dadd_rn(s0 * s0, s1 * s1) : s0 * s0;
+                    const double nn = sqrt(__dadd_rn(n2rows, kz2));
+                    const int b = (int)nn;
+                    if (b >= bc.nbins) continue;
+                    if (b != cur) {
+                        if (cur >= 0) {
+                            atomicAdd(&pw[cur], ap);
+                            if (BINS == 2) {
+                                atomicAdd(&ws[cur], aw);
+                                atomicAdd(&ks[cur], ak);
+                            }
+                        }
+                        cur = b;
+                        ap = aw = ak = 0.0;
+                    }
+                    const double2 f = buf[tr(k0, cc)];
+                    const double kc = __dmul_rn(nn, bc.dk);
+                    double kd = kc;
+                    if (bc.d >= 2) kd = __dmul_rn(kd, kc);
+                    if (bc.d == 3) kd = __dmul_rn(kd, kc);
+                    const double mag = __dadd_rn(__dmul_rn(f.x, f.x), __dmul_rn(f.y, f.y));
+                    ap = __dadd_rn(ap, __dmul_rn(__dmul_rn(__dmul_rn(wp, kd), bc.pnorm), mag));
+                    if (BINS == 2) {
+                        aw = __dadd_rn(aw, w);
+                        ak = __dadd_rn(ak, __dmul_rn(w, kc));
+                    }
+                }
+                if (cur >= 0) {
+                    atomicAdd(&pw[cur], ap);
+                    if (BINS == 2) {
+                        atomicAdd(&ws[cur], aw);
+                        atomicAdd(&ks[cur], ak);
+                    }
+                }
+            }
+        }
+    }
+    if constexpr (BINS) {
+        __syncthreads();
+        double *out = hist + (size_t)blockIdx.x * NH * bc.nbins;
+        for (int i = threadIdx.x; i < NH * bc.nbins; i += blockDim.x) out[i] = hs[i];
+    }
+}
+
 
 /* Shell sums of bubble.cpp:680-701 per block: smem histograms, then one row
  * of partials per block. A warp takes a row of the half-complex array in
@@ -370,7 +662,7 @@ __global__ void __launch_bounds__(FFT_T) k_bins(BinConst bc, const double2 *__re
             const double s0 = (double)sidx((long long)q, bc.n), s1 = (double)sidx((long long)m, bc.n);
             n2rows = __dadd_rn(s0 * s0, s1 * s1);
         }
-        const double2 *row = half + (size_t)r * bc.h;
+        const double2 *row = half + (size_t)r * bc.pitch;
         for (int c0 = 0; c0 < bc.h; c0 += BIN_CHUNK) {
             /* the shell index grows with the column: a chunk that starts beyond the
              * last shell ends the row (the same for every lane of the warp) */
@@ -503,10 +795,16 @@ std::vector<double2> twiddles(int n) {
     return w;
 }
 
-int fft_setup(cb_handle *h, FftState *&out, int d, int n, cudaStream_t s) {
+/* The register-resident forward kernels cover d = 2, 3 with n a power of two, 64 <= n <= 512. */
+bool reg_shape(int d, int n) { return (d == 2 || d == 3) && n >= 64 && n <= 512 && (n & (n - 1)) == 0; }
+
+/* forward: the state serves forward transforms (the register-resident kernels
+ * where the shape allows, with the padded row pitch) */
+int fft_setup(cb_handle *h, FftState *&out, int d, int n, cudaStream_t s, bool forward = false) {
     FftState *f = new FftState();
     f->n = n;
     f->d = d;
+    f->reg = forward && reg_shape(d, n);
     if (n > MAX_FFT_N || !factor(n, f->radix, f->nstages)) {
         delete f;
         return fail(h, CB_EUNSUPPORTED, "power spectrum: n_grids must be at most 6144 and have prime factors <= 13");
@@ -514,7 +812,8 @@ int fft_setup(cb_handle *h, FftState *&out, int d, int n, cudaStream_t s) {
     const int hh = n / 2 + 1;
     size_t rows = 1;
     for (int i = 0; i < d - 1; ++i) rows *= (size_t)n;
-    f->half_elems = rows * hh;
+    f->pitch = f->reg ? (hh + PITCH_ALIGN - 1) / PITCH_ALIGN * PITCH_ALIGN : hh;
+    f->half_elems = rows * f->pitch;
     f->nbins = (int)(std::sqrt(double(d)) * n / 2) + 1;
     f->hist_blocks = 148 * 4;
     std::vector<double2> w = twiddles(n);
@@ -523,6 +822,8 @@ int fft_setup(cb_handle *h, FftState *&out, int d, int n, cudaStream_t s) {
     if (e == cudaSuccess) e = cudaMallocAsync(&f->hist, (size_t)f->hist_blocks * 3 * f->nbins * sizeof(double), s);
     if (e == cudaSuccess) e = cudaMallocAsync(&f->bins_out, 3 * (size_t)f->nbins * sizeof(double), s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(f->tw, w.data(), n * sizeof(double2), cudaMemcpyHostToDevice, s);
+    /* the pad columns are transformed with the others: zeros keep them finite */
+    if (e == cudaSuccess && f->pitch != hh) e = cudaMemsetAsync(f->half, 0, f->half_elems * sizeof(double2), s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -538,8 +839,97 @@ int fft_setup(cb_handle *h, FftState *&out, int d, int n, cudaStream_t s) {
     return CB_OK;
 }
 
+int sm_count();
+
+/* Resident blocks of a persistent register-FFT kernel (at least one per SM). */
+template <typename K>
+unsigned reg_grid(K kern, int threads, size_t smem, unsigned ntiles) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    const unsigned g = (unsigned)per_sm * (unsigned)sm_count();
+    return g < ntiles ? g : ntiles;
+}
+
+/* r2c by the register-resident kernels (f->reg): rows, then the leading axes.
+ * With bins, the last axis also bins |phi_k|^2 (per-block histograms, then
+ * k_bins_reduce into f->bins_out) and the transform of that axis is not kept. */
+template <int N>
+cudaError_t fft_r2c_reg_n(FftState *f, int prec, const void *field, cudaStream_t s, const BinConst *bins) {
+    constexpr int RC = rc_of(N), threads = N / 8 * RC;
+    const int d = f->d;
+    size_t rows = 1;
+    for (int i = 0; i < d - 1; ++i) rows *= (size_t)N;
+    const unsigned row_tiles = (unsigned)(rows / (2 * RC));
+    const size_t sm_rows = 2 * (size_t)RC * (N + N / 8) * sizeof(double2);
+    cudaError_t e;
+    if (prec == P_FP64) {
+        auto k = k_fft_rows_reg<double, N>;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_rows)) != cudaSuccess)
+            return e;
+        k<<<reg_grid(k, threads, sm_rows, row_tiles), threads, sm_rows, s>>>((const double *)field, row_tiles,
+                                                                             f->pitch, f->tw, f->half);
+    } else {
+        auto k = k_fft_rows_reg<float, N>;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_rows)) != cudaSuccess)
+            return e;
+        k<<<reg_grid(k, threads, sm_rows, row_tiles), threads, sm_rows, s>>>((const float *)field, row_tiles,
+                                                                             f->pitch, f->tw, f->half);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const size_t sm_cols = 2 * (size_t)col_buf(N, RC) * sizeof(double2);
+    /* the mode counts and k sums are binned once per state (they depend on the lattice alone) */
+    const int nh = f->geom_done ? 1 : 3;
+    const size_t sm_bins = sm_cols + (bins ? nh * (size_t)bins->nbins * sizeof(double) : 0);
+    if ((e = cudaFuncSetAttribute(k_fft_cols_reg<0, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sm_cols)) != cudaSuccess)
+        return e;
+    for (int ax = d - 2; ax >= 0; --ax) {
+        size_t outer = 1, inner = (size_t)f->pitch;
+        for (int i = 0; i < ax; ++i) outer *= (size_t)N;
+        for (int i = ax + 1; i < d - 1; ++i) inner *= (size_t)N;
+        const unsigned tiles = (unsigned)(outer * (inner / RC));
+        if (bins && ax == 0) {
+            auto k = f->geom_done ? k_fft_cols_reg<1, N> : k_fft_cols_reg<2, N>;
+            if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_bins)) != cudaSuccess)
+                return e;
+            unsigned g = reg_grid(k, threads, sm_bins, tiles);
+            if (g > (unsigned)f->hist_blocks) g = (unsigned)f->hist_blocks;
+            k<<<g, threads, sm_bins, s>>>(f->half, tiles, inner, f->tw, *bins, f->hist);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            /* the power (and on the first call the counts and k sums) into bins_out */
+            const int width = nh * bins->nbins;
+            k_bins_reduce<<<(width + 31) / 32, 256, 0, s>>>(f->hist, (int)g, width, f->bins_out);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            f->geom_done = true;
+        } else {
+            auto k = k_fft_cols_reg<0, N>;
+            k<<<reg_grid(k, threads, sm_cols, tiles), threads, sm_cols, s>>>(f->half, tiles, inner, f->tw, BinConst{},
+                                                                             nullptr);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+/* r2c by the register-resident kernels (f->reg): rows, then the leading axes.
+ * With bins, the last axis also bins |phi_k|^2 (per-block histograms, then
+ * k_bins_reduce into f->bins_out) and the transform of that axis is not kept. */
+cudaError_t fft_r2c_reg(FftState *f, int prec, const void *field, cudaStream_t s, const BinConst *bins = nullptr) {
+    switch (f->n) {
+        case 64: return fft_r2c_reg_n<64>(f, prec, field, s, bins);
+        case 128: return fft_r2c_reg_n<128>(f, prec, field, s, bins);
+        case 256: return fft_r2c_reg_n<256>(f, prec, field, s, bins);
+        case 512: return fft_r2c_reg_n<512>(f, prec, field, s, bins);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 /* r2c of `field` (n^d values of the given precision) into f->half. */
 cudaError_t fft_r2c(FftState *f, int prec, const void *field, cudaStream_t s) {
+    if (f->reg) return fft_r2c_reg(f, prec, field, s);
     const int n = f->n, d = f->d;
     Plan pl = plan_of(*f);
     size_t rows = 1;
@@ -599,19 +989,25 @@ cudaError_t fft_c2r(FftState *f, double *out, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t fft_bins(FftState *f, double L, cudaStream_t s) {
+BinConst bin_const(const FftState *f, double L) {
     const int n = f->n, d = f->d;
     BinConst bc;
     bc.d = d;
     bc.n = n;
     bc.h = n / 2 + 1;
+    bc.pitch = f->pitch;
     bc.nbins = f->nbins;
-    bc.rows = f->half_elems / bc.h;
+    bc.rows = f->half_elems / f->pitch;
     bc.dk = 2.0 * M_PI / L;                                   /* bubble.cpp:672 */
     bc.pref = (d == 1) ? 1.0 / M_PI : (d == 2) ? 1.0 / (2.0 * M_PI) : 1.0 / (2.0 * M_PI * M_PI);   /* :673 */
     const double dx = L / n;
     const double dxD = std::pow(dx, d);                        /* bubble.hpp:46 */
     bc.pnorm = dxD * dxD / std::pow(L, d);                     /* bubble.cpp:674 */
+    return bc;
+}
+
+cudaError_t fft_bins(FftState *f, double L, cudaStream_t s) {
+    const BinConst bc = bin_const(f, L);
     const size_t sm = 3 * (size_t)bc.nbins * sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(k_bins, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
@@ -636,11 +1032,17 @@ extern "C" int cb_power_spectrum(cb_handle *h, double *power, double *weight, do
         if (r != CB_OK) return r;
         if (!h->fft) {
             FftState *f = nullptr;
-            if ((r = fft_setup(h, f, h->p.d, h->p.n_grids, h->stream)) != CB_OK) return r;
+            if ((r = fft_setup(h, f, h->p.d, h->p.n_grids, h->stream, true)) != CB_OK) return r;
             h->fft = f;
         }
-        cudaError_t e = fft_r2c(h->fft, h->prec, h->phi[h->cphi], h->stream);
-        if (e == cudaSuccess) e = fft_bins(h->fft, h->p.L, h->stream);
+        cudaError_t e;
+        if (h->fft->reg) {
+            const BinConst bc = bin_const(h->fft, h->p.L);
+            e = fft_r2c_reg(h->fft, h->prec, h->phi[h->cphi], h->stream, &bc);
+        } else {
+            e = fft_r2c(h->fft, h->prec, h->phi[h->cphi], h->stream);
+            if (e == cudaSuccess) e = fft_bins(h->fft, h->p.L, h->stream);
+        }
         std::vector<double> host(3 * (size_t)nb);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(host.data(), h->fft->bins_out, host.size() * sizeof(double), cudaMemcpyDeviceToHost,
@@ -711,14 +1113,16 @@ extern "C" int cb_dft_r2c(int d, int n, const double *in, double *out) {
         cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
         if (e != cudaSuccess) return cuda_fail(nullptr, e, "creating a stream");
         FftState *f = nullptr;
-        int r = fft_setup(nullptr, f, d, n, s);
+        int r = fft_setup(nullptr, f, d, n, s, true);
         if (r != CB_OK) { cudaStreamDestroy(s); return r; }
         double *dev = nullptr;
         e = cudaMalloc(&dev, N * sizeof(double));
         if (e == cudaSuccess) e = cudaMemcpyAsync(dev, in, N * sizeof(double), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = fft_r2c(f, P_FP64, dev, s);
+        const size_t hh = (size_t)n / 2 + 1;
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(out, f->half, f->half_elems * sizeof(double2), cudaMemcpyDeviceToHost, s);
+            e = cudaMemcpy2DAsync(out, hh * sizeof(double2), f->half, (size_t)f->pitch * sizeof(double2),
+                                  hh * sizeof(double2), f->half_elems / f->pitch, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         cudaFree(dev);
         cudaFreeAsync(f->tw, s); cudaFreeAsync(f->half, s); cudaFreeAsync(f->hist, s); cudaFreeAsync(f->bins_out, s);

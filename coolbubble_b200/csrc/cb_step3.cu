@@ -77,6 +77,22 @@ struct Cursor {
     }
 };
 
+/* Kahan-compensated accumulator of packed float pairs (each half its own
+ * compensated sum; the two are added in double at the end). */
+struct AccF2 {
+    F2 s{0ull}, c{0ull};
+    __device__ __forceinline__ void add(F2 x) {
+        const F2 y = f2_sub(x, c);
+        const F2 t = f2_add(s, y);
+        c = f2_sub(f2_sub(t, s), y);
+        s = t;
+    }
+    __device__ __forceinline__ double value() const {
+        return __dadd_rn(__dsub_rn((double)f2_lo(s), (double)f2_lo(c)),
+                         __dsub_rn((double)f2_hi(s), (double)f2_hi(c)));
+    }
+};
+
 /* Shared-memory layout of one stage: phi rows [TJ + 2][n] (row 0 and TJ + 1
  * are the halo rows), then pi rows [TJ + 2*DF][n] (drift-first also needs the
  * halo rows of pi to drift the halo of phi). */
@@ -150,7 +166,8 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
     pdl_wait();          /* the previous step's fields, device state and work queue */
 
     Acc<T> acc[NSUM];
-    F2 pacc[NSUM];   /* float path: plain pair sums (the sums that are not compensated) */
+    AccF2 kacc[NSUM];   /* float path: the compensated sums (energies) */
+    F2 pacc[NSUM];      /* float path: plain pair sums (averages; squares by fused multiply-add) */
 
     if (warp == CW) {
         /* ---- producer warp: lane 0 takes items from the queue and issues the
@@ -265,9 +282,17 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
             for (int v = threadIdx.x; v < nv_drift; v += NC) {
                 VT f = *reinterpret_cast<const VT *>(S + v * W);
                 const VT mom = *reinterpret_cast<const VT *>(Pi + v * W);
+                if constexpr (PACKED) {
+                    /* the same three roundings per site, two sites per instruction */
+                    const F2 P_P = f2_splat((float)p);
+                    const F2 f01 = f2_add(f2_pack(f.x, f.y), f2_mul(f2_mul(P_DT, f2_pack(mom.x, mom.y)), P_P));
+                    const F2 f23 = f2_add(f2_pack(f.z, f.w), f2_mul(f2_mul(P_DT, f2_pack(mom.z, mom.w)), P_P));
+                    f = make_float4(f2_lo(f01), f2_hi(f01), f2_lo(f23), f2_hi(f23));
+                } else {
 #pragma unroll
-                for (int t = 0; t < W; ++t)
-                    Vec<T>::set(f, t, A::add(Vec<T>::get(f, t), A::mul(A::mul(dt, Vec<T>::get(mom, t)), p)));
+                    for (int t = 0; t < W; ++t)
+                        Vec<T>::set(f, t, A::add(Vec<T>::get(f, t), A::mul(A::mul(dt, Vec<T>::get(mom, t)), p)));
+                }
                 *reinterpret_cast<VT *>(S + v * W) = f;
             }
             /* every consumer thread arrives once its own share is written */
@@ -308,6 +333,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
 #pragma unroll
                 for (int s = 0; s < NSUM; ++s) {
                     acc[s] = Acc<T>{};
+                    kacc[s] = AccF2{};
                     pacc[s] = f2_splat(0.f);
                 }
             }
@@ -400,16 +426,17 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                                 v[S_EG] = eg;
                             }
                             if constexpr (SUMS == SUM_FULL) {
+                                /* the Q_ slots carry the values whose squares are summed
+                                 * (squared and added in one fused multiply-add below) */
                                 const F2 vv = f2_mul(pi_n, P_VW);
-                                const F2 et = f2_add(f2_add(ek, eg), ep);
                                 v[S_PHI] = cc;
                                 v[S_V] = vv;
-                                v[Q_EK] = f2_mul(ek, ek);
-                                v[Q_EP] = f2_mul(ep, ep);
-                                v[Q_EG] = f2_mul(eg, eg);
-                                v[Q_ET] = f2_mul(et, et);
-                                v[Q_PHI] = f2_mul(cc, cc);   /* the same product as in V(f) */
-                                v[Q_V] = f2_mul(vv, vv);
+                                v[Q_EK] = ek;
+                                v[Q_EP] = ep;
+                                v[Q_EG] = eg;
+                                v[Q_ET] = f2_add(f2_add(ek, eg), ep);
+                                v[Q_PHI] = cc;
+                                v[Q_V] = vv;
                                 v[S_EKIN_IN] = f2_mul(f2_mul(P_KW, pp), pp);
                             }
                         }
@@ -424,15 +451,18 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                         constexpr int NA = SUMS == SUM_FULL ? NSUM : (want_eg ? 3 : 2);
 #pragma unroll
                         for (int q = 0; q < NA; ++q) {
-                            const F2 t = f2_add(v01[q], v23[q]);
                             /* the energies (and the previous half step's kinetic sum, which
-                             * enters the time-centred Ekin) are compensated; the field
-                             * averages and the sums of squares behind the spreads are plain
-                             * float sums of pairs over the item's vectors (a few dozen per
-                             * thread at 512^3, restarted with every item: relative error
-                             * ~1e-6) */
-                            if (q == S_EK || q == S_EP || q == S_EG || q == S_EKIN_IN) acc[q].add(f2_lo(t) + f2_hi(t));
-                            else pacc[q] = f2_add(pacc[q], t);
+                             * enters the time-centred Ekin) are compensated, per half of the
+                             * pair; the field averages and the sums of squares behind the
+                             * spreads are plain float sums over the item's vectors (a few
+                             * dozen per thread at 512^3, restarted with every item: relative
+                             * error ~1e-6), the squares added by fused multiply-adds */
+                            if (q == S_EK || q == S_EP || q == S_EG || q == S_EKIN_IN)
+                                kacc[q].add(f2_add(v01[q], v23[q]));
+                            else if (q >= Q_EK && q <= Q_V)
+                                pacc[q] = f2_fma(v23[q], v23[q], f2_fma(v01[q], v01[q], pacc[q]));
+                            else
+                                pacc[q] = f2_add(pacc[q], f2_add(v01[q], v23[q]));
                         }
                         if constexpr (SUMS == SUM_FULL) {
                             vek = make_float4(f2_lo(v01[S_EK]), f2_hi(v01[S_EK]), f2_lo(v23[S_EK]), f2_hi(v23[S_EK]));
@@ -557,7 +587,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                 for (int s = 0; s < NS; ++s) {
                     double x = acc[s].value();
                     if constexpr (std::is_same<T, float>::value)
-                        x = __dadd_rn(x, __dadd_rn((double)f2_lo(pacc[s]), (double)f2_hi(pacc[s])));
+                        x = __dadd_rn(kacc[s].value(), __dadd_rn((double)f2_lo(pacc[s]), (double)f2_hi(pacc[s])));
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));
                     if (lane == 0) item_red[j & 1][warp][s] = x;

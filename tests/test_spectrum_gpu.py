@@ -26,7 +26,9 @@ def dft(d, n, x):
 
 
 @pytest.mark.parametrize("d,n", [(1, 64), (1, 30), (1, 1000), (2, 48), (2, 96), (2, 384), (2, 100), (3, 12),
-                                 (3, 16), (3, 64), (3, 192), (2, 28), (2, 39)])
+                                 (3, 16), (3, 64), (3, 192), (2, 28), (2, 39),
+                                 # the register-resident kernels (powers of two, 64 .. 512)
+                                 (2, 64), (2, 128), (2, 256), (2, 512), (3, 128), (3, 256)])
 def test_dft_matches_numpy(d, n):
     rng = np.random.default_rng(d * 1000 + n)
     x = rng.standard_normal((n,) * d)
@@ -62,6 +64,8 @@ def test_spectrum_matches_reference_golden(name):
     dict(d=2, n=512, L=32.0, c=4.0, ic="bubbles"),
     dict(d=2, n=384, L=48.0, c=3.0, ic="bubbles"),
     dict(d=3, n=128, L=32.0, c=2.0, ic="noise"),
+    dict(d=3, n=64, L=16.0, c=2.0, ic="noise"),
+    dict(d=2, n=64, L=16.0, c=4.0, ic="bubbles"),
     dict(d=3, n=96, L=24.0, c=4.0, ic="bubbles", expansion=1, mpl=10.0),
     dict(d=1, n=2048, L=64.0, c=4.0, ic="noise"),
 ])
