@@ -203,7 +203,9 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
         if (lane == 0) {
             int q = 0;
             bool ok = true;
-            int cur = (int)atomicAdd(&st->item_next, 1u);
+            /* the first item of every block is its own index (the grid never
+             * exceeds the items); later ones come from the queue */
+            int cur = (int)blockIdx.x;
             for (int j = 0; ok; ++j) {
                 /* hand item j (or the end of the queue) to the consumers; the
                  * queue slot was read IQ items ago: every item streams at least
@@ -231,7 +233,7 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                 /* the next item is taken only now, with this one fully issued:
                  * taken earlier, a block would hold back an item an idle block
                  * could run (the consumers still have the ring's planes to do) */
-                if (ok) cur = (int)atomicAdd(&st->item_next, 1u);
+                if (ok) cur = (int)gridDim.x + (int)atomicAdd(&st->item_next, 1u);
             }
             issued_count = q;
         }
@@ -617,18 +619,22 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
             cq = cp;
         }
     }
+    __threadfence();   /* this block's fields and partial rows, before its count below */
     __syncthreads();
     /* this block's items are done: the next step may be scheduled (its blocks
      * take the slots the finished blocks leave, and wait for this grid) */
     pdl_allow_next();
-    /* the last block out resets the work queue for the next launch on the stream */
+    /* one count per block: the last block out resets the work queue for the
+     * next launch on the stream and runs the sums' epilogue */
+    __shared__ bool is_last;
     if (threadIdx.x == 0) {
-        __threadfence();
-        if (atomicAdd(&st->item_done, 1u) == gridDim.x - 1) {
+        is_last = atomicAdd(&st->item_done, 1u) == gridDim.x - 1;
+        if (is_last) {
             st->item_next = 0u;
             st->item_done = 0u;
         }
     }
+    __syncthreads();
     if (abort_flag) {
         /* record, then let every issued copy land before the block exits */
         if (threadIdx.x == 0) {
@@ -643,7 +649,8 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
 
     if (SUMS != SUM_NONE) {
         __shared__ double tot[NSUM];
-        if (last_block_ticket<NT3>(&st->counter)) {
+        if (is_last) {
+            __threadfence();   /* every block's rows are counted: read them after this */
             sum_rows<NT3, NS>(partials, (unsigned)items, tot);
             if (threadIdx.x < 32) epilogue(k, st, tot, !DF, SUMS == SUM_FULL, threadIdx.x);
         }

@@ -253,7 +253,9 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
     int is_stage = 0;                                            /* its stage: issued mod nstage */
     bool pr_done = false;
     auto next_item = [&]() {
-        const int cur = (int)atomicAdd(&st->item_next, 1u);
+        /* a block's first item is its own index (the grid never exceeds the
+         * items); later ones come from the queue */
+        const int cur = pr_j == 0 ? (int)blockIdx.x : (int)gridDim.x + (int)atomicAdd(&st->item_next, 1u);
         pr_it = cur < items ? cur : -1;
         item_q[pr_j % TB_IQ] = pr_it;
         ++pr_j;
