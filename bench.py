@@ -426,9 +426,12 @@ def measure_lattice(w, prec, K, W, phi_h, pi_h, dist=None, clocks=None, spectra=
     ws = 1 if dist is None else dist.get_world_size()
     peak, _ = measured_peak()
     per_launch = ms / launches
-    alg = BYTES_PER_SITE[prec] * N
+    # HBM passes over the lattice: a static launch is one pass (of one or two
+    # steps); an expanding step is one pass, also inside a multi-step launch
+    passes = K if w["expansion"] else launches
+    alg = BYTES_PER_SITE[prec] * N * passes / launches
     achieved = alg / (per_launch / 1e3) / 1e9
-    out = dict(value=N * K * ws / (ms / 1e3), ms=ms, ms_per_step=ms / K, launches=launches, warmup=Wp,
+    out = dict(value=N * K * ws / (ms / 1e3), ms=ms, ms_per_step=ms / K, launches=launches, passes=passes, warmup=Wp,
                per_launch_ms=per_launch, alg_bytes=alg, achieved_gbs=achieved, frac=achieved / peak,
                effective_gbs=N * K * BYTES_PER_SITE[prec] / (ms / 1e3) / 1e9, clocks=clk, final=final,
                spectrum_ms=spec)
@@ -595,7 +598,8 @@ def lattice_summary(m, prec):
     return {"value": m["value"], "unit": "site-updates/s", "precision": prec, "ms_per_step": m["ms_per_step"],
             "steps": round(m["ms"] / m["ms_per_step"]), "warmup": m["warmup"],
             "roofline": {"bound": "hbm", "achieved": m["achieved_gbs"], "frac": m["frac"], "unit": "GB/s",
-                         "alg_bytes_per_launch": m["alg_bytes"], "launch_ms": m["per_launch_ms"]},
+                         "alg_bytes_per_launch": m["alg_bytes"], "launch_ms": m["per_launch_ms"],
+                         "passes_per_launch": m["passes"] / m["launches"]},
             "effective_frac": m["effective_frac"], "plain_step_ms": m.get("plain_step_ms"),
             "sums_step_ms": m.get("sums_step_ms"), "spectrum_ms": m.get("spectrum_ms")}
 

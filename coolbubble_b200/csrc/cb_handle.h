@@ -60,6 +60,7 @@ struct cb_handle {
     /* replayable chains of plain steps (small lattices), by (cphi, cpi) at their start */
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     bool graphs_off = false;
+    bool multi_off = false;  /* multi-step launches unavailable (or CB_MULTI_STEP=0) */
     std::string err;
 };
 

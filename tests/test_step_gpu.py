@@ -336,6 +336,34 @@ def test_step_graphs_equal_plain_launches(d, n, prec, expansion, monkeypatch):
         np.testing.assert_array_equal(fa[key], fb[key])
 
 
+@pytest.mark.parametrize("n,alpha", [(64, 0), (128, 0), (256, 0), (128, 1)])
+def test_multi_step_launch_equals_single_launches(n, alpha, monkeypatch):
+    """Runs of plain expanding float steps in one cooperative launch (every
+    block forming the Friedmann update itself after a bounded grid barrier)
+    give the fields, sums, time and background of one launch per step, bit
+    for bit, in fewer launches."""
+    import coolbubble_b200 as cb
+    L = n / 8.0
+    p = cb.make_params(3, n, L, 4.0, 0.1 * L / n, expansion=1, mpl=10.0, alpha=alpha, precision="fp32c",
+                       memorysave=1)
+    phi0 = bubbles(3, n, L, 4.0, 4, seed=11)
+    pi0 = smooth_noise(3, n, 0.02, seed=12)
+    multi = cb.Bubble(p, phi0, pi0)
+    monkeypatch.setenv("CB_MULTI_STEP", "0")
+    single = cb.Bubble(p, phi0, pi0)
+    for steps in (40, 17, 2, 1, 33):
+        monkeypatch.delenv("CB_MULTI_STEP")
+        a = multi.step(steps, sums=True)
+        monkeypatch.setenv("CB_MULTI_STEP", "0")
+        b = single.step(steps, sums=True)
+        assert a == b, steps
+    (lm, nm), (ls_, ns) = multi.counters(), single.counters()
+    assert nm == ns == 93 and lm < ls_
+    fa, fb = multi.fields(), single.fields()
+    for key in fa:
+        np.testing.assert_array_equal(fa[key], fb[key])
+
+
 def test_fp64_tiled_static_matches_oracle():
     import coolbubble_b200 as cb
     from oracle import bridge as B
