@@ -461,7 +461,10 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                 } else {
                     bad = !(acquire(cm) && acquire(c0));
                 }
-                for (int i = p0; !bad && i < p1; ++i) {
+                /* multi-step launches: two planes per loop trip (256^3: 0.0523 ->
+             * 0.0514 ms per step); the one-launch variants measured slower so */
+#pragma unroll(MS ? 2 : 1)
+            for (int i = p0; !bad && i < p1; ++i) {
                     if (DF ? !drifted_wait(cp) : !acquire(cp)) {
                         bad = true;
                         break;

@@ -402,6 +402,10 @@ __global__ void __launch_bounds__(TB_MAXT, 1)
         if (end_round(g, bad)) break;
         ++g;
         advance();
+        /* two rounds per loop trip: the register queues of period two (input
+         * phi, level-1 pi) then trade places without moves (512^3: 0.2288 ->
+         * 0.2225 ms per step; no spills at 128 registers) */
+#pragma unroll 2
         for (int q = p0; q <= p1 + 1; ++q, ++g, advance()) {
             if (!bad && acquire()) {
                 const uint32_t Sn = ring_a + gs * stage_b;        /* plane q */
