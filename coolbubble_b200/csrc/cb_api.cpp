@@ -479,17 +479,17 @@ int step_impl(cb_handle *h, int nsteps, int flags, bool timed) {
     const int tl = h->k.temporal;
     const bool tb_ok = !h->expanding && h->unit_scale && tl > 1 &&
                        step3tb_geometry(h->k, h->prec, tl, tj, ns, sm, g, parts);
-    /* expanding float 3-D: runs of plain steps in one cooperative launch */
+    /* expanding 3-D: runs of plain steps in one cooperative launch */
     const char *ms_env = std::getenv("CB_MULTI_STEP");
-    const bool ms_ok = h->expanding && h->prec == P_FP32 && h->k.d == 3 && !h->k.force_generic && !h->multi_off &&
+    const bool ms_ok = h->expanding && h->k.d == 3 && !h->k.force_generic && !h->multi_off &&
                        !(ms_env && ms_env[0] == '0');
     for (int it = 1; it <= nsteps;) {
         const int plain_left = nsteps - it + 1 - (want_last ? 1 : 0);
         if (ms_ok && !h->multi_off && plain_left >= 2) {
             const int m = std::min(plain_left, MULTI_STEP_MAX);
             const int i = h->cphi, j = h->cpi;
-            e = launch_step3_ms(h->k, m, h->phi[i], h->pi[j], h->phi[1 - i], h->pi[1 - j], h->st, h->partials,
-                                h->stream);
+            e = launch_step3_ms(h->prec, h->k, m, h->phi[i], h->pi[j], h->phi[1 - i], h->pi[1 - j], h->st,
+                                h->partials, h->stream);
             if (e == cudaErrorNotSupported) {
                 cudaGetLastError();
                 h->multi_off = true;   /* steps one launch each from now on */

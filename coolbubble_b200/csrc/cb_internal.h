@@ -136,8 +136,8 @@ size_t step3_partial_rows(const StepConst &k, int prec);
 cudaError_t launch_step3(int prec, const StepConst &k, bool drift_first, int sums, const void *phi_in,
                          const void *pi_in, void *phi_out, void *pi_out, void *loc_ek, void *loc_eg, void *loc_ep,
                          DevState *st, double *partials, cudaStream_t s);
-cudaError_t launch_step3_ms(const StepConst &k, int nsteps, void *phi_a, void *pi_a, void *phi_b, void *pi_b,
-                            DevState *st, double *partials, cudaStream_t s);
+cudaError_t launch_step3_ms(int prec, const StepConst &k, int nsteps, void *phi_a, void *pi_a, void *phi_b,
+                            void *pi_b, DevState *st, double *partials, cudaStream_t s);
 
 /* TL steps per pass, static float 3-D lattices (cb_step3_tb.cu). */
 bool step3tb_geometry(const StepConst &k, int prec, int tl, int &tj, int &nstage, size_t &smem, unsigned &grid,

@@ -171,8 +171,8 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                                                 const T *phi_in, const T *pi_in, T *phi_out, T *pi_out,
                                                 T *__restrict__ loc_ek, T *__restrict__ loc_eg,
                                                 T *__restrict__ loc_ep, DevState *st, double *partials) {
-    static_assert(!MS || (DF && std::is_same<T, float>::value && (SUMS == SUM_FRIEDMANN || SUMS == SUM_FRIEDMANN_EG)),
-                  "multi-step launches cover drift-first float steps with the Friedmann sums");
+    static_assert(!MS || (DF && (SUMS == SUM_FRIEDMANN || SUMS == SUM_FRIEDMANN_EG)),
+                  "multi-step launches cover drift-first steps with the Friedmann sums");
     using A = Ar<T>;
     using VT = typename Vec<T>::V;
     constexpr int W = Vec<T>::W;
@@ -461,9 +461,10 @@ __global__ void __launch_bounds__(NT3, 2) k_step3(StepConst k, int tj, int nstag
                 } else {
                     bad = !(acquire(cm) && acquire(c0));
                 }
-                /* multi-step launches: two planes per loop trip (256^3: 0.0523 ->
-             * 0.0514 ms per step); the one-launch variants measured slower so */
-#pragma unroll(MS ? 2 : 1)
+                /* float multi-step launches: two planes per loop trip (256^3:
+             * 0.0523 -> 0.0514 ms per step); the one-launch variants measured
+             * slower so */
+#pragma unroll(MS && std::is_same<T, float>::value ? 2 : 1)
             for (int i = p0; !bad && i < p1; ++i) {
                     if (DF ? !drifted_wait(cp) : !acquire(cp)) {
                         bad = true;
@@ -943,12 +944,13 @@ cudaError_t launch_step3(int prec, const StepConst &k, bool df, int sums, const 
  * end in B for odd nsteps). cudaErrorNotSupported where the staged kernel
  * does not apply or its blocks cannot all be resident (the caller then
  * launches the steps one by one). */
-cudaError_t launch_step3_ms(const StepConst &k, int nsteps, void *phi_a, void *pi_a, void *phi_b, void *pi_b,
-                            DevState *st, double *partials, cudaStream_t s) {
+template <typename T>
+cudaError_t launch_step3_ms_t(int prec, const StepConst &k, int nsteps, void *phi_a, void *pi_a, void *phi_b,
+                              void *pi_b, DevState *st, double *partials, cudaStream_t s) {
     int tj, nstage, parts;
     size_t smem;
     unsigned grid;
-    if (!k.expanding || k.d != 3 || nsteps < 1 || !step3_geometry_parts(k, P_FP32, tj, nstage, smem, grid, parts))
+    if (!k.expanding || k.d != 3 || nsteps < 1 || !step3_geometry_parts(k, prec, tj, nstage, smem, grid, parts))
         return cudaErrorNotSupported;
     /* only where a step is one round of items (every block one item): there
      * the launch gap and the ramp of each step are what a multi-step launch
@@ -956,7 +958,7 @@ cudaError_t launch_step3_ms(const StepConst &k, int nsteps, void *phi_a, void *p
      * with several rounds per step one launch per step measured faster
      * (384^3: 0.165 against 0.179 ms, 512^3: 0.393 against 0.404) */
     if ((long long)(k.n / tj) * parts > (long long)grid) return cudaErrorNotSupported;
-    auto fn = k.alpha == 1 ? k_step3<float, true, SUM_FRIEDMANN_EG, true> : k_step3<float, true, SUM_FRIEDMANN, true>;
+    auto fn = k.alpha == 1 ? k_step3<T, true, SUM_FRIEDMANN_EG, true> : k_step3<T, true, SUM_FRIEDMANN, true>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -973,11 +975,16 @@ cudaError_t launch_step3_ms(const StepConst &k, int nsteps, void *phi_a, void *p
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, fn, k, tj, nstage, parts, nsteps, (const float *)phi_a, (const float *)pi_a,
-                           (float *)phi_b, (float *)pi_b, (float *)nullptr, (float *)nullptr, (float *)nullptr, st,
-                           partials);
+    e = cudaLaunchKernelEx(&cfg, fn, k, tj, nstage, parts, nsteps, (const T *)phi_a, (const T *)pi_a, (T *)phi_b,
+                           (T *)pi_b, (T *)nullptr, (T *)nullptr, (T *)nullptr, st, partials);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
+}
+
+cudaError_t launch_step3_ms(int prec, const StepConst &k, int nsteps, void *phi_a, void *pi_a, void *phi_b,
+                            void *pi_b, DevState *st, double *partials, cudaStream_t s) {
+    return prec == P_FP64 ? launch_step3_ms_t<double>(prec, k, nsteps, phi_a, pi_a, phi_b, pi_b, st, partials, s)
+                          : launch_step3_ms_t<float>(prec, k, nsteps, phi_a, pi_a, phi_b, pi_b, st, partials, s);
 }
 
 }  // namespace cb

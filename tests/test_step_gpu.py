@@ -336,15 +336,16 @@ def test_step_graphs_equal_plain_launches(d, n, prec, expansion, monkeypatch):
         np.testing.assert_array_equal(fa[key], fb[key])
 
 
-@pytest.mark.parametrize("n,alpha", [(64, 0), (128, 0), (256, 0), (128, 1)])
-def test_multi_step_launch_equals_single_launches(n, alpha, monkeypatch):
-    """Runs of plain expanding float steps in one cooperative launch (every
+@pytest.mark.parametrize("n,alpha,prec", [(64, 0, "fp32c"), (128, 0, "fp32c"), (256, 0, "fp32c"), (128, 1, "fp32c"),
+                                          (128, 0, "fp64"), (128, 1, "fp64")])
+def test_multi_step_launch_equals_single_launches(n, alpha, prec, monkeypatch):
+    """Runs of plain expanding steps in one cooperative launch (every
     block forming the Friedmann update itself after a bounded grid barrier)
     give the fields, sums, time and background of one launch per step, bit
     for bit, in fewer launches."""
     import coolbubble_b200 as cb
     L = n / 8.0
-    p = cb.make_params(3, n, L, 4.0, 0.1 * L / n, expansion=1, mpl=10.0, alpha=alpha, precision="fp32c",
+    p = cb.make_params(3, n, L, 4.0, 0.1 * L / n, expansion=1, mpl=10.0, alpha=alpha, precision=prec,
                        memorysave=1)
     phi0 = bubbles(3, n, L, 4.0, 4, seed=11)
     pi0 = smooth_noise(3, n, 0.02, seed=12)
